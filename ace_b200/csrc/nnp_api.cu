@@ -1,0 +1,667 @@
+// nnp_api.cu -- the C ABI of libnnp_b200.so (declared in include/nnp_b200.h).
+//
+// A handle holds a parsed potential (host copy, for writing it back and for
+// parameter get/set), its device form, one stream and the scratch buffers.
+// No entry point throws: errors come back as NNP_ERR_* codes with a message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/nnp_b200.h"
+#include "nnp_engine.h"
+
+struct nnp_handle {
+    nnp::Engine E;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(nnp_handle *h, int code, const std::string &msg)
+{
+    if (h) h->E.last_error = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+bool read_file(const char *path, std::string &out)
+{
+    std::ifstream f(path, std::ios::in | std::ios::binary);
+    if (!f) return false;
+    std::ostringstream ss;
+    ss << f.rdbuf();
+    out = ss.str();
+    return true;
+}
+
+bool is_pinned_or_device(const void *p, bool *device)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        *device = false;
+        return false;
+    }
+    *device = (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged);
+    return a.type == cudaMemoryTypeHost || *device;
+}
+
+}  // namespace
+
+namespace nnp {
+
+void Engine::free_all()
+{
+    rpar.release(); apar.release(); wpar.release(); vac.release();
+    atom_off.release(); pos.release(); cell.release(); xw.release();
+    type.release(); atom_struct.release(); atom_cell.release(); grid.release();
+    cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
+    nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
+    e_struct.release(); force.release(); symm_d.release(); err.release();
+    if (d_pot) cudaFree(d_pot);
+    d_pot = nullptr;
+    if (h_err) cudaFreeHost(h_err);
+    h_err = nullptr;
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
+    h_stage_bytes = 0;
+    if (own_stream && stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    own_stream = false;
+}
+
+// Build the device potential.  Angular functions of one BasisA that form a
+// run of equal eta (BasisA::init, basis_angular.cpp:178-205) share the run's
+// first eta for their damping factor, as the reference does.
+std::string Engine::upload()
+{
+    const HostPot &H = host;
+    const int T = H.ntypes();
+    DevPot d;
+    std::memset(&d, 0, sizeof d);
+    d.ntypes = T;
+    d.rc = (float)H.rc;
+    d.rc_d = H.rc;
+    std::vector<std::pair<int, double>> cuts;
+    auto cut_id = [&](int name, double rc) -> int {
+        for (size_t k = 0; k < cuts.size(); ++k)
+            if (cuts[k].first == name && cuts[k].second == rc) return (int)k;
+        if ((int)cuts.size() >= NNP_MAX_CUT) return -1;
+        cuts.push_back({name, rc});
+        return (int)cuts.size() - 1;
+    };
+    std::vector<float2> rp;
+    std::vector<float4> ap;
+    std::vector<float> wp;
+    std::vector<double> vc(T);
+    for (int II = 0; II < T; ++II) {
+        DevType &t = d.t[II];
+        t.n_input = H.n_input(II);
+        t.n_input_r = H.n_input_r(II);
+        int off = 0;
+        for (int J = 0; J < T; ++J) {
+            const HostBasisR &b = H.br[II][J];
+            const int n = (int)b.rs.size();
+            if (n > NNP_MAX_RFUNC) return "a radial basis has more functions than the device path supports";
+            const int c = cut_id(b.cut, b.rc);
+            if (c < 0) return "too many distinct cutoffs in the potential";
+            t.br[J] = {n, off, b.form, c, (int)rp.size()};
+            for (int f = 0; f < n; ++f) rp.push_back(make_float2((float)b.rs[f], (float)b.eta[f]));
+            off += n;
+        }
+        int offa = t.n_input_r;
+        t.ndamp = 0;
+        const int TT = T * (T + 1) / 2;
+        for (int tt = 0; tt < TT; ++tt) {
+            const HostBasisA &b = H.ba[II][tt];
+            const int n = (int)b.eta.size();
+            if (n > NNP_MAX_AFUNC) return "an angular basis has more functions than the device path supports";
+            const int c = cut_id(b.cut, b.rc);
+            if (c < 0) return "too many distinct cutoffs in the potential";
+            int int_zeta = 1;
+            double etar = n ? b.eta[0] : 0.0;
+            for (int f = 0; f < n; ++f) {
+                if (f > 0 && std::fabs(b.eta[f] - b.eta[f - 1]) >= 1.0e-6) etar = b.eta[f];
+                const double a = 1.0 / (etar * etar);
+                int dmp = 0;
+                if (b.form == ANG_GAUSS) {
+                    dmp = -1;
+                    for (int k = 0; k < t.ndamp; ++k)
+                        if (t.damp_cut[k] == c && t.damp_a[k] == (float)a) dmp = k;
+                    if (dmp < 0) {
+                        if (t.ndamp >= NNP_MAX_DAMP) return "too many distinct angular widths for one element";
+                        t.damp_cut[t.ndamp] = c;
+                        t.damp_a[t.ndamp] = (float)a;
+                        dmp = t.ndamp++;
+                    }
+                }
+                const double z = b.zeta[f];
+                const int iz = (z == std::floor(z) && z >= 0.0 && z <= 64.0) ? (int)z : -1;
+                if (iz < 0) int_zeta = 0;
+                const int pk = dmp | ((iz + 1) << 8);
+                float w;
+                std::memcpy(&w, &pk, sizeof w);
+                ap.push_back(make_float4((float)(0.5 * b.lambda[f]), (float)z, (float)a, w));
+            }
+            t.ba[tt] = {n, offa, b.form, c, (int)ap.size() - n, int_zeta};
+            offa += n;
+        }
+        // network
+        const HostNet &net = H.nets[II];
+        t.nlayer = (int)net.nodes.size() - 1;
+        if (t.nlayer > NNP_MAX_LAYERS) return "network has more layers than the device path supports";
+        for (size_t l = 0; l < net.nodes.size(); ++l) {
+            if (net.nodes[l] > NNP_MAX_NODES) return "network layer wider than the device path supports";
+            t.nodes[l] = net.nodes[l];
+        }
+        t.neuron = net.neuron;
+        t.c = (float)net.c;
+        t.woff = (int64_t)wp.size();
+        for (double x : net.inpw) wp.push_back((float)x);
+        for (double x : net.inpb) wp.push_back((float)x);
+        for (double x : net.outw) wp.push_back((float)x);
+        for (double x : net.outb) wp.push_back((float)x);
+        for (int l = 0; l < t.nlayer; ++l) {
+            const int ni = net.nodes[l], no = net.nodes[l + 1], s = wt_stride(no);
+            for (int n = 0; n < no; ++n) wp.push_back((float)net.b[l][n]);
+            const size_t base = wp.size();
+            wp.resize(base + (size_t)ni * s, 0.f);
+            for (int n = 0; n < no; ++n)
+                for (int m = 0; m < ni; ++m) wp[base + (size_t)m * s + n] = (float)net.w[l][(size_t)n * ni + m];
+        }
+        vc[II] = H.types[II].energy;
+    }
+    d.ncut = (int)cuts.size();
+    for (size_t k = 0; k < cuts.size(); ++k) {
+        d.cut[k].name = cuts[k].first;
+        d.cut[k].rc = (float)cuts[k].second;
+        d.cut[k].rci = (float)(1.0 / cuts[k].second);
+        d.cut[k].pirci = (float)(3.141592653589793 / cuts[k].second);
+    }
+    int gs = 1;
+    for (int II = 0; II < T; ++II) gs = std::max(gs, d.t[II].n_input);
+    gstride = (gs + 3) & ~3;
+    wfloats = (int64_t)wp.size();
+    dpot = d;
+    if (rp.empty()) rp.push_back(make_float2(0.f, 0.f));
+    if (ap.empty()) ap.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+    cudaError_t e = cudaSuccess;
+    auto r = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
+    if (!d_pot) r(cudaMalloc((void **)&d_pot, sizeof(DevPot)));
+    r(rpar.reserve(rp.size()));
+    r(apar.reserve(ap.size()));
+    r(wpar.reserve(wp.size()));
+    r(vac.reserve(vc.size()));
+    if (e != cudaSuccess) return std::string("device allocation failed: ") + cudaGetErrorString(e);
+    r(cudaMemcpy(d_pot, &d, sizeof d, cudaMemcpyHostToDevice));
+    r(cudaMemcpy(rpar.p, rp.data(), rp.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(apar.p, ap.data(), ap.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(wpar.p, wp.data(), wp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(vac.p, vc.data(), vc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (e != cudaSuccess) return std::string("potential upload failed: ") + cudaGetErrorString(e);
+    return "";
+}
+
+}  // namespace nnp
+
+namespace {
+
+int finish_create(nnp_handle *h, nnp_handle **out)
+{
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        cudaGetLastError();
+        delete h;
+        return fail(nullptr, NNP_ERR_CUDA, "no CUDA device available: the NNP path runs only on the GPU");
+    }
+    nnp::Engine &E = h->E;
+    if (cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return fail(nullptr, NNP_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    E.own_stream = true;
+    if (cudaMallocHost((void **)&E.h_err, sizeof(nnp::DevErr)) != cudaSuccess) {
+        E.free_all();
+        delete h;
+        return fail(nullptr, NNP_ERR_CUDA, "cudaMallocHost failed");
+    }
+    std::string msg = E.upload();
+    if (!msg.empty()) {
+        E.free_all();
+        delete h;
+        return fail(nullptr, NNP_ERR_CUDA, msg);
+    }
+    E.cap = 64;
+    *out = h;
+    return NNP_OK;
+}
+
+// pinned staging: copy host data through the handle's pinned buffer unless
+// it is already pinned (or device) memory
+int stage_bytes(nnp::Engine &E, size_t bytes)
+{
+    if (bytes <= E.h_stage_bytes) return NNP_OK;
+    if (E.h_stage) cudaFreeHost(E.h_stage);
+    E.h_stage = nullptr;
+    E.h_stage_bytes = 0;
+    const size_t want = bytes + bytes / 4 + 4096;
+    if (cudaMallocHost(&E.h_stage, want) != cudaSuccess) return NNP_ERR_CUDA;
+    E.h_stage_bytes = want;
+    return NNP_OK;
+}
+
+cudaError_t h2d(nnp::Engine &E, void *dst, const void *src, size_t bytes, size_t &stage_off)
+{
+    if (!bytes) return cudaSuccess;
+    bool dev = false;
+    if (is_pinned_or_device(src, &dev)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, E.stream);
+    char *st = (char *)E.h_stage + stage_off;
+    std::memcpy(st, src, bytes);
+    stage_off += (bytes + 255) & ~(size_t)255;
+    return cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, E.stream);
+}
+
+int estimate_cap(const nnp_batch *b, double rc)
+{
+    double pmax = 16.0;
+    for (int s = 0; s < b->n_struct; ++s) {
+        const int64_t n = b->atom_off[s + 1] - b->atom_off[s];
+        if (n <= 0) continue;
+        double p;
+        if (b->pbc) {
+            const double *c = b->cell + 9 * (int64_t)s;
+            const double V = std::fabs(c[0] * (c[4] * c[8] - c[5] * c[7]) - c[1] * (c[3] * c[8] - c[5] * c[6]) +
+                                       c[2] * (c[3] * c[7] - c[4] * c[6]));
+            p = V > 0 ? 4.18879020478639 * rc * rc * rc * (double)n / V : 256.0;
+        } else {
+            p = (double)(n - 1);
+        }
+        pmax = std::max(pmax, p);
+    }
+    int cap = (int)std::ceil(1.5 * pmax + 24.0);
+    cap = (cap + 7) & ~7;
+    return std::min(cap, NNP_MAX_NBR);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *nnp_version(void) { return "nnp_b200 0.1 (sm_100a)"; }
+
+const char *nnp_last_error(const nnp_handle *h) { return h ? h->E.last_error.c_str() : g_create_error.c_str(); }
+
+int nnp_create_from_file(const char *path, nnp_handle **out)
+{
+    if (!path || !out) return fail(nullptr, NNP_ERR_ARG, "nnp_create_from_file: null argument");
+    *out = nullptr;
+    std::string text;
+    if (!read_file(path, text))
+        return fail(nullptr, NNP_ERR_IO, std::string("NNP::read(const char*,NNP&): Could not open nnp file: \"") + path + "\"");
+    nnp_handle *h = new nnp_handle();
+    std::string msg = nnp::read_potential(text, h->E.host);
+    if (!msg.empty()) {
+        delete h;
+        return fail(nullptr, NNP_ERR_PARSE, msg);
+    }
+    return finish_create(h, out);
+}
+
+int nnp_create_from_basis(int32_t ntypes, const char *const *type_lines, double rc, const char *const *basis_paths,
+                          const char *const *network_texts, nnp_handle **out)
+{
+    if (!out || !type_lines || !basis_paths || !network_texts || ntypes <= 0)
+        return fail(nullptr, NNP_ERR_ARG, "nnp_create_from_basis: bad argument");
+    if (ntypes > NNP_MAX_TYPES) return fail(nullptr, NNP_ERR_UNSUPPORTED, "too many element types");
+    if (!(rc > 0)) return fail(nullptr, NNP_ERR_ARG, "NNP::read(FILE*,NNP&): invalid cutoff.");
+    *out = nullptr;
+    // a minimal potential text with empty bases, then fill in the pieces
+    std::string text = "ann\nntypes " + std::to_string(ntypes) + "\n";
+    for (int i = 0; i < ntypes; ++i) text += std::string(type_lines[i]) + "\n";
+    nnp_handle *h = new nnp_handle();
+    nnp::HostPot &P = h->E.host;
+    {
+        // parse types with the potential parser by appending an empty rest
+        std::istringstream is(text);
+        std::string ln;
+        std::getline(is, ln);
+        std::getline(is, ln);
+        P.types.resize(ntypes);
+        for (int i = 0; i < ntypes; ++i) {
+            std::getline(is, ln);
+            std::istringstream ts(ln);
+            std::vector<std::string> tok;
+            std::string t;
+            while (ts >> t) tok.push_back(t);
+            P.types[i].name = "NONE";
+            for (size_t k = 0; k + 1 < tok.size(); k += 2) {
+                std::string tag = tok[k];
+                for (auto &c : tag) c = (char)toupper((unsigned char)c);
+                const double v = std::atof(tok[k + 1].c_str());
+                if (tag == "NAME") P.types[i].name = tok[k + 1];
+                else if (tag == "ENERGY") P.types[i].energy = v;
+                else if (tag == "MASS") P.types[i].mass = v;
+                else if (tag == "CHARGE") P.types[i].charge = v;
+                else if (tag == "RADIUS") P.types[i].radius = v;
+                else if (tag == "Z") P.types[i].z = v;
+                else if (tag == "ALPHA") P.types[i].alpha = v;
+                else if (tag == "IE") P.types[i].ie = v;
+                else if (tag == "RCOV") P.types[i].rcov = v;
+                else if (tag == "RVDW") P.types[i].rvdw = v;
+                else if (tag == "AMP") P.types[i].amp = v;
+            }
+        }
+    }
+    P.rc = rc;
+    P.br.assign(ntypes, std::vector<nnp::HostBasisR>(ntypes));
+    P.ba.assign(ntypes, std::vector<nnp::HostBasisA>(ntypes * (ntypes + 1) / 2));
+    P.nets.assign(ntypes, nnp::HostNet());
+    for (int i = 0; i < ntypes; ++i) {
+        std::string btxt;
+        if (!read_file(basis_paths[i], btxt)) {
+            delete h;
+            return fail(nullptr, NNP_ERR_IO, std::string("NNP::read_basis(const char*,NNP&,const char*): Could not open nnp file: \"") + basis_paths[i] + "\"");
+        }
+        std::string msg = nnp::read_basis_file(btxt, P, i);
+        if (msg.empty()) msg = nnp::read_network(network_texts[i], P.nets[i]);
+        if (msg.empty() && P.nets[i].nodes.front() != P.n_input(i)) msg = "network input size differs from the basis size";
+        if (!msg.empty()) {
+            delete h;
+            return fail(nullptr, NNP_ERR_PARSE, msg);
+        }
+    }
+    return finish_create(h, out);
+}
+
+int nnp_destroy(nnp_handle *h)
+{
+    if (!h) return NNP_OK;
+    h->E.free_all();
+    delete h;
+    return NNP_OK;
+}
+
+int nnp_write(const nnp_handle *h, const char *path)
+{
+    if (!h || !path) return NNP_ERR_ARG;
+    std::ofstream f(path, std::ios::out | std::ios::binary);
+    if (!f) return fail(const_cast<nnp_handle *>(h), NNP_ERR_IO, std::string("NNP::write(const char*,const NNP&): Could not write to nnh file: \"") + path + "\"");
+    f << nnp::write_potential(h->E.host);
+    return NNP_OK;
+}
+
+int nnp_set_precision(nnp_handle *h, int32_t precision)
+{
+    if (!h) return NNP_ERR_ARG;
+    if (precision != NNP_PREC_FP32 && precision != NNP_PREC_BF16 && precision != NNP_PREC_BF16X3)
+        return fail(h, NNP_ERR_ARG, "unknown precision");
+    h->E.precision = precision;
+    return NNP_OK;
+}
+
+int nnp_set_stream(nnp_handle *h, void *cuda_stream)
+{
+    if (!h) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (E.own_stream && E.stream) cudaStreamDestroy(E.stream);
+    E.own_stream = false;
+    E.stream = (cudaStream_t)cuda_stream;
+    if (!E.stream) {
+        cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
+        E.own_stream = true;
+    }
+    return NNP_OK;
+}
+
+int nnp_ntypes(const nnp_handle *h, int32_t *ntypes)
+{
+    if (!h || !ntypes) return NNP_ERR_ARG;
+    *ntypes = h->E.host.ntypes();
+    return NNP_OK;
+}
+
+int nnp_type_index(const nnp_handle *h, const char *name, int32_t *index)
+{
+    if (!h || !name || !index) return NNP_ERR_ARG;
+    for (int i = 0; i < h->E.host.ntypes(); ++i)
+        if (h->E.host.types[i].name == name) {
+            *index = i;
+            return NNP_OK;
+        }
+    *index = -1;
+    return fail(const_cast<nnp_handle *>(h), NNP_ERR_TYPE, std::string("unknown element ") + name);
+}
+
+int nnp_rc(const nnp_handle *h, double *rc)
+{
+    if (!h || !rc) return NNP_ERR_ARG;
+    *rc = h->E.host.rc;
+    return NNP_OK;
+}
+
+int nnp_n_input(const nnp_handle *h, int32_t type, int32_t *n_input)
+{
+    if (!h || !n_input || type < 0 || type >= h->E.host.ntypes()) return NNP_ERR_ARG;
+    *n_input = h->E.host.n_input(type);
+    return NNP_OK;
+}
+
+int nnp_nparams(const nnp_handle *h, int32_t type, int32_t *n)
+{
+    if (!h || !n) return NNP_ERR_ARG;
+    if (type < 0) {
+        int s = 0;
+        for (const auto &net : h->E.host.nets) s += net.nparams();
+        *n = s;
+        return NNP_OK;
+    }
+    if (type >= h->E.host.ntypes()) return NNP_ERR_ARG;
+    *n = h->E.host.nets[type].nparams();
+    return NNP_OK;
+}
+
+int nnp_get_params(const nnp_handle *h, double *params)
+{
+    if (!h || !params) return NNP_ERR_ARG;
+    size_t k = 0;
+    for (const auto &net : h->E.host.nets) {
+        const int nl = (int)net.nodes.size() - 1;
+        for (int l = 0; l < nl; ++l)
+            for (double v : net.b[l]) params[k++] = v;
+        for (int l = 0; l < nl; ++l) {
+            const int ni = net.nodes[l], no = net.nodes[l + 1];
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) params[k++] = net.w[l][(size_t)n * ni + m];
+        }
+    }
+    return NNP_OK;
+}
+
+int nnp_set_params(nnp_handle *h, const double *params)
+{
+    if (!h || !params) return NNP_ERR_ARG;
+    size_t k = 0;
+    for (auto &net : h->E.host.nets) {
+        const int nl = (int)net.nodes.size() - 1;
+        for (int l = 0; l < nl; ++l)
+            for (auto &v : net.b[l]) v = params[k++];
+        for (int l = 0; l < nl; ++l) {
+            const int ni = net.nodes[l], no = net.nodes[l + 1];
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) net.w[l][(size_t)n * ni + m] = params[k++];
+        }
+    }
+    std::string msg = h->E.upload();
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    return NNP_OK;
+}
+
+int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out, uint32_t flags)
+{
+    if (!h || !b) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (b->n_struct < 0) return fail(h, NNP_ERR_ARG, "negative structure count");
+    if ((flags & NNP_ENERGY) && !energy) return fail(h, NNP_ERR_ARG, "energy output missing");
+    if ((flags & NNP_FORCES) && !forces) return fail(h, NNP_ERR_ARG, "force output missing");
+    if ((flags & NNP_SYMM) && !symm_out) return fail(h, NNP_ERR_ARG, "symmetry-function output missing");
+    if (E.precision != NNP_PREC_FP32) return fail(h, NNP_ERR_UNSUPPORTED, "this build implements the FP32 network path only");
+    const int S = b->n_struct;
+    if (S == 0) return NNP_OK;
+    if (!b->atom_off || !b->pos || !b->type || (b->pbc && !b->cell)) return fail(h, NNP_ERR_ARG, "batch array missing");
+    const bool devp = (flags & NNP_DEVICE_PTRS) != 0;
+    int64_t N = 0;
+    cudaError_t ce = cudaSuccess;
+    auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
+    if (!devp) {
+        if (b->atom_off[0] != 0) return fail(h, NNP_ERR_ARG, "atom_off[0] must be 0");
+        for (int s = 0; s < S; ++s)
+            if (b->atom_off[s + 1] < b->atom_off[s]) return fail(h, NNP_ERR_ARG, "atom_off must be non-decreasing");
+        N = b->atom_off[S];
+        if (N >= (int64_t)1 << 28) return fail(h, NNP_ERR_CAPACITY, "more than 2^28 atoms in one batch");
+        const int T = E.host.ntypes();
+        for (int64_t i = 0; i < N; ++i)
+            if (b->type[i] < 0 || b->type[i] >= T)
+                return fail(h, NNP_ERR_TYPE, "atom " + std::to_string(i) + " has type index " + std::to_string(b->type[i]) + " outside [0," + std::to_string(T) + ")");
+        E.cap = std::max(E.cap, estimate_cap(b, E.host.rc));
+        // inputs -> device
+        const size_t bo = sizeof(int64_t) * (S + 1), bp = sizeof(double) * 3 * N, bt = sizeof(int32_t) * N,
+                     bc = b->pbc ? sizeof(double) * 9 * S : 0;
+        if (stage_bytes(E, bo + bp + bt + bc + 4 * 256) != NNP_OK) return fail(h, NNP_ERR_CUDA, "cudaMallocHost failed");
+        chk(E.atom_off.reserve(S + 1));
+        chk(E.pos.reserve(3 * std::max<int64_t>(N, 1)));
+        chk(E.type.reserve(std::max<int64_t>(N, 1)));
+        chk(E.cell.reserve(9 * (size_t)S));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
+        size_t so = 0;
+        chk(h2d(E, E.atom_off.p, b->atom_off, bo, so));
+        chk(h2d(E, E.pos.p, b->pos, bp, so));
+        chk(h2d(E, E.type.p, b->type, bt, so));
+        if (b->pbc) chk(h2d(E, E.cell.p, b->cell, bc, so));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("input copy failed: ") + cudaGetErrorString(ce));
+    } else {
+        int64_t n = 0;
+        chk(cudaMemcpyAsync(&n, b->atom_off + S, sizeof n, cudaMemcpyDeviceToHost, E.stream));
+        chk(cudaStreamSynchronize(E.stream));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("reading atom count failed: ") + cudaGetErrorString(ce));
+        N = n;
+        if (N < 0 || N >= (int64_t)1 << 28) return fail(h, NNP_ERR_ARG, "bad atom count in atom_off");
+        if (E.cap < 128) E.cap = 128;
+        // run on the caller's arrays in place
+    }
+    // kernels read through these
+    nnp::DBuf<int64_t> u_off = E.atom_off;
+    nnp::DBuf<double> u_pos = E.pos, u_cell = E.cell;
+    nnp::DBuf<int> u_type = E.type;
+    if (devp) {
+        E.atom_off.p = const_cast<int64_t *>(b->atom_off);
+        E.pos.p = const_cast<double *>(b->pos);
+        E.type.p = const_cast<int32_t *>(b->type);
+        E.cell.p = const_cast<double *>(b->cell);
+    }
+    int rc = NNP_OK;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::string msg = nnp::run_prepare(E, N, S, b->pbc);
+        if (msg.empty()) msg = nnp::run_neighbors(E, b->pbc);
+        if (msg.empty()) msg = nnp::run_symm(E);
+        if (msg.empty() && (flags & (NNP_ENERGY | NNP_FORCES))) msg = nnp::run_nn(E);
+        if (msg.empty() && (flags & NNP_FORCES)) msg = nnp::run_force(E);
+        if (msg.empty() && (flags & NNP_ENERGY)) msg = nnp::run_energy(E, (flags & NNP_VACUUM) != 0);
+        if (!msg.empty()) { rc = fail(h, NNP_ERR_CUDA, msg); break; }
+        chk(cudaMemcpyAsync(E.h_err, E.err.p, sizeof(nnp::DevErr), cudaMemcpyDeviceToHost, E.stream));
+        chk(cudaStreamSynchronize(E.stream));
+        if (ce != cudaSuccess) { rc = fail(h, NNP_ERR_CUDA, std::string("kernel failure: ") + cudaGetErrorString(ce)); break; }
+        const nnp::DevErr er = *E.h_err;
+        if (er.bad_type) { rc = fail(h, NNP_ERR_TYPE, "atom type index out of range"); break; }
+        if (er.bad_cell) { rc = fail(h, NNP_ERR_ARG, "a periodic cell has zero volume"); break; }
+        if (er.need_cap > E.cap) {
+            if (er.need_cap > NNP_MAX_NBR) {
+                rc = fail(h, NNP_ERR_CAPACITY, "an atom has " + std::to_string(er.need_cap) + " neighbours; the device path handles up to " + std::to_string(NNP_MAX_NBR));
+                break;
+            }
+            E.cap = std::min(NNP_MAX_NBR, ((er.need_cap + er.need_cap / 8 + 8) + 7) & ~7);
+            continue;
+        }
+        if (er.nonfinite) { rc = fail(h, NNP_ERR_NOT_FINITE, "non-finite energy or force"); }
+        // outputs
+        if (!devp) {
+            const size_t be = sizeof(double) * S, bf = sizeof(double) * 3 * N;
+            if (flags & NNP_ENERGY) chk(cudaMemcpyAsync(energy, E.e_struct.p, be, cudaMemcpyDeviceToHost, E.stream));
+            if (flags & NNP_FORCES) chk(cudaMemcpyAsync(forces, E.force.p, bf, cudaMemcpyDeviceToHost, E.stream));
+            if (flags & NNP_SYMM) {
+                chk(E.symm_d.reserve((size_t)N * E.gstride + 1));
+                nnp::run_symm_to_double(E, E.symm_d.p);
+                chk(cudaMemcpyAsync(symm_out, E.symm_d.p, sizeof(double) * N * E.gstride, cudaMemcpyDeviceToHost, E.stream));
+            }
+        } else {
+            if (flags & NNP_ENERGY) chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToDevice, E.stream));
+            if (flags & NNP_FORCES) chk(cudaMemcpyAsync(forces, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, E.stream));
+            if (flags & NNP_SYMM) nnp::run_symm_to_double(E, symm_out);
+        }
+        chk(cudaStreamSynchronize(E.stream));
+        if (ce != cudaSuccess) rc = fail(h, NNP_ERR_CUDA, std::string("output copy failed: ") + cudaGetErrorString(ce));
+        break;
+    }
+    if (devp) {
+        E.atom_off = u_off;
+        E.pos = u_pos;
+        E.cell = u_cell;
+        E.type = u_type;
+    }
+    return rc;
+}
+
+int nnp_compute_energy_symm(nnp_handle *h, int32_t n_struct, const int64_t *atom_off, const int32_t *type,
+                            const double *symm, int32_t gstride, double *energy)
+{
+    if (!h || !atom_off || !type || !symm || !energy || n_struct < 0) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (n_struct == 0) return NNP_OK;
+    const int64_t N = atom_off[n_struct];
+    const int T = E.host.ntypes();
+    for (int64_t i = 0; i < N; ++i)
+        if (type[i] < 0 || type[i] >= T) return fail(h, NNP_ERR_TYPE, "atom type index out of range");
+    if (gstride < E.gstride) {
+        // repack to the device row length
+    }
+    cudaError_t ce = cudaSuccess;
+    auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
+    std::string msg = nnp::run_prepare(E, N, n_struct, 0);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    chk(E.atom_off.reserve(n_struct + 1));
+    chk(E.type.reserve(std::max<int64_t>(N, 1)));
+    chk(E.symm_d.reserve((size_t)std::max<int64_t>(N, 1) * E.gstride));
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, "device allocation failed");
+    std::vector<double> rows((size_t)N * E.gstride, 0.0);
+    for (int64_t i = 0; i < N; ++i)
+        for (int g = 0; g < std::min<int>(gstride, E.gstride); ++g) rows[(size_t)i * E.gstride + g] = symm[(size_t)i * gstride + g];
+    chk(cudaMemcpyAsync(E.atom_off.p, atom_off, sizeof(int64_t) * (n_struct + 1), cudaMemcpyHostToDevice, E.stream));
+    chk(cudaMemcpyAsync(E.type.p, type, sizeof(int32_t) * N, cudaMemcpyHostToDevice, E.stream));
+    chk(cudaMemcpyAsync(E.symm_d.p, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice, E.stream));
+    msg = nnp::run_nn_from_symm(E, E.symm_d.p, E.gstride);
+    if (msg.empty()) msg = nnp::run_energy(E, true);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * n_struct, cudaMemcpyDeviceToHost, E.stream));
+    chk(cudaStreamSynchronize(E.stream));
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("compute_energy failed: ") + cudaGetErrorString(ce));
+    return NNP_OK;
+}
+
+int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, const double *f_ref, double w_f,
+                   int32_t norm_mode, double *loss, double *grad, double *e_out, double *f_out, uint32_t flags)
+{
+    (void)batch; (void)e_ref; (void)f_ref; (void)w_f; (void)norm_mode; (void)loss; (void)grad; (void)e_out;
+    (void)f_out; (void)flags;
+    if (!h) return NNP_ERR_ARG;
+    return fail(h, NNP_ERR_UNSUPPORTED, "nnp_train_grad is not built yet");
+}
+
+}  // extern "C"

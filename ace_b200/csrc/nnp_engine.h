@@ -1,0 +1,111 @@
+// nnp_engine.h -- device buffers of one handle and the launch sequence of the
+// energy/force path.  Used by the C ABI (nnp_api.cu); kernels live in
+// nnp_kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "nnp_internal.h"
+
+namespace nnp {
+
+// per-structure neighbour-search grid (filled on the device)
+struct StructGrid {
+    double R[9];      // R[3n+d]: component d of lattice vector n
+    double B[9];      // B[3n+d]: reciprocal row n (fractional coordinate n = B_n . x)
+    int nc[3];        // cells per lattice direction
+    int m[3];         // cells searched on each side
+    int cell_base;    // first global cell index of this structure
+    int pbc;
+};
+
+// device error record: kernels raise flags, the host reads them after a step
+struct DevErr {
+    int need_cap;     // largest neighbour count seen (when above the capacity)
+    int bad_type;     // an atom type was outside [0, ntypes)
+    int bad_cell;     // a periodic cell had no volume
+    int nonfinite;    // a non-finite energy or force
+};
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t reserve(size_t count)
+    {
+        if (count <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        size_t c = count + count / 4 + 16;
+        cudaError_t e = cudaMalloc((void **)&p, c * sizeof(T));
+        if (e == cudaSuccess) n = c;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Engine {
+    // potential
+    HostPot host;
+    DevPot dpot{};
+    DevPot *d_pot = nullptr;
+    DBuf<float2> rpar;            // radial (rs, eta)
+    DBuf<float4> apar;            // angular (lambdaf, zeta, ieta2, damp | izeta << 8)
+    DBuf<float> wpar;             // networks, FP32 (layout in nnp_internal.h)
+    DBuf<double> vac;             // per-type vacuum energies
+    int64_t wfloats = 0;
+    int gstride = 0;              // row length of G / dE/dG (max n_input rounded up to 4)
+    int precision = 0;
+
+    // stream / events
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // batch
+    int n_struct = 0;
+    int64_t n_atoms = 0;
+    int cap = 0;                  // neighbour slots per atom
+    int tot_cells = 0;
+    DBuf<int64_t> atom_off;
+    DBuf<double> pos, cell, xw;
+    DBuf<int> type, atom_struct, atom_cell;
+    DBuf<StructGrid> grid;
+    DBuf<int> cell_cnt, cell_start, cell_fill, cell_atoms, scan_tmp;
+    DBuf<float4> nbr;
+    DBuf<int> nbr_cnt;
+    DBuf<float> G, dEdG, e_atom;
+    DBuf<double> e_struct, force, symm_d;
+    DBuf<DevErr> err;
+    DevErr *h_err = nullptr;      // pinned
+    // pinned staging for host-pointer calls
+    void *h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+
+    std::string last_error;
+
+    // build the device potential from `host`
+    std::string upload();
+    void free_all();
+};
+
+// launch sequence (nnp_kernels.cu); each returns "" or an error message
+std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc);
+std::string run_neighbors(Engine &E, int pbc);
+std::string run_symm(Engine &E);
+std::string run_nn(Engine &E);
+std::string run_force(Engine &E);
+std::string run_energy(Engine &E, bool vacuum);
+std::string run_symm_to_double(Engine &E, double *out);
+std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
+
+}  // namespace nnp

@@ -1,0 +1,1047 @@
+// nnp_kernels.cu -- the energy/force path on sm_100a.
+//
+// Stages (one launch each, all on the handle's stream):
+//   k_atom_struct  atom -> structure map (binary search of the CSR offsets)
+//   k_struct_setup per-structure cell grid in lattice coordinates
+//   k_cell_base    exclusive scan of cells per structure
+//   k_bin          wrap atoms into their cell, count atoms per cell
+//   k_cell_start   per-structure scan of the cell counts
+//   k_fill, k_sort_cells   cell member lists, sorted by atom index
+//   k_neigh        one warp per atom: candidates from the (2m+1)^3 cells,
+//                  exact FP64 displacement test, neighbours grouped by type
+//                  (replaces NeighborList::build, struc/neighbor.cpp:46-87)
+//   k_symm         one warp per atom: radial + angular symmetry functions
+//                  (NNP::compute_symm, nnp/nnp.cpp:350-392)
+//   k_nn_fp32      one warp per atom: network forward + input gradient dE/dG
+//                  (ANN::fpbp + DODZ::grad, ml/nn.cpp:1402-1420,1836-1859)
+//   k_force        one warp per atom: adjoint of the symmetry functions,
+//                  per-neighbour gradients, FP64 force scatter
+//                  (NNP::compute_force, nnp/nnp.cpp:412-476)
+//   k_energy       one block per structure, FP64 energy sum
+#include <cstdio>
+
+#include "nnp_engine.h"
+#include "nnp_math.cuh"
+
+namespace nnp {
+
+#define FULL 0xffffffffu
+#define WARPS 8
+#define SYMM_CHUNK 8   // angular functions accumulated in registers per pass
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+
+static int grid_for(int64_t items, int per_block, int max_blocks)
+{
+    int64_t b = (items + per_block - 1) / per_block;
+    if (b < 1) b = 1;
+    if (b > max_blocks) b = max_blocks;
+    return (int)b;
+}
+
+static std::string cuda_msg(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return "";
+    return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+// ------------------------------------------------------------------ structure grids
+
+__global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N, int *__restrict__ atom_struct,
+                              const int *__restrict__ type, int ntypes, DevErr *err)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int lo = 0, hi = S - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    atom_struct[i] = lo;
+    const int t = type[i];
+    if (t < 0 || t >= ntypes) atomicMax(&err->bad_type, 1);
+}
+
+__global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *__restrict__ off, int S, int pbc,
+                               double rc, StructGrid *__restrict__ grid, int *__restrict__ ncells, DevErr *err)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    StructGrid g;
+    const int64_t nat = off[s + 1] - off[s];
+    for (int k = 0; k < 9; ++k) { g.R[k] = 0.0; g.B[k] = 0.0; }
+    g.nc[0] = g.nc[1] = g.nc[2] = 1;
+    g.m[0] = g.m[1] = g.m[2] = 0;
+    g.pbc = pbc;
+    g.cell_base = 0;
+    if (pbc) {
+        for (int k = 0; k < 9; ++k) g.R[k] = cell[9 * (int64_t)s + k];
+        const double *a[3] = {g.R, g.R + 3, g.R + 6};
+        double c[3][3];
+        for (int n = 0; n < 3; ++n) {
+            const double *p = a[(n + 1) % 3], *q = a[(n + 2) % 3];
+            c[n][0] = p[1] * q[2] - p[2] * q[1];
+            c[n][1] = p[2] * q[0] - p[0] * q[2];
+            c[n][2] = p[0] * q[1] - p[1] * q[0];
+        }
+        const double V = a[0][0] * c[0][0] + a[0][1] * c[0][1] + a[0][2] * c[0][2];
+        if (!(fabs(V) > 1e-12)) {
+            atomicMax(&err->bad_cell, 1);
+            g.pbc = 0;
+        } else {
+            double w[3];
+            for (int n = 0; n < 3; ++n) {
+                for (int d = 0; d < 3; ++d) g.B[3 * n + d] = c[n][d] / V;
+                w[n] = fabs(V) / sqrt(c[n][0] * c[n][0] + c[n][1] * c[n][1] + c[n][2] * c[n][2]);
+                int nc = (int)floor(w[n] / rc);
+                g.nc[n] = nc < 1 ? 1 : (nc > 1024 ? 1024 : nc);
+            }
+            const int64_t lim = nat * 2 > 64 ? nat * 2 : 64;
+            while ((int64_t)g.nc[0] * g.nc[1] * g.nc[2] > lim) {
+                int k = 0;
+                if (g.nc[1] > g.nc[k]) k = 1;
+                if (g.nc[2] > g.nc[k]) k = 2;
+                g.nc[k] = (g.nc[k] + 1) / 2;
+            }
+            for (int n = 0; n < 3; ++n) g.m[n] = (int)ceil(rc * g.nc[n] / w[n]);
+        }
+    }
+    grid[s] = g;
+    ncells[s] = g.nc[0] * g.nc[1] * g.nc[2];
+}
+
+// exclusive scan of ncells over structures in one block; writes cell_base
+__global__ void k_cell_base(const int *__restrict__ ncells, int S, StructGrid *__restrict__ grid)
+{
+    __shared__ int part[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int chunk = (S + T - 1) / T;
+    const int b = t * chunk, e = min(S, b + chunk);
+    int s = 0;
+    for (int k = b; k < e; ++k) s += ncells[k];
+    part[t] = s;
+    __syncthreads();
+    for (int d = 1; d < T; d <<= 1) {
+        const int v = (t >= d) ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = part[t] - s;
+    for (int k = b; k < e; ++k) {
+        grid[k].cell_base = run;
+        run += ncells[k];
+    }
+}
+
+__global__ void k_bin(int64_t N, const double *__restrict__ pos, const int *__restrict__ atom_struct,
+                      const StructGrid *__restrict__ grid, double *__restrict__ xw, int *__restrict__ atom_cell,
+                      int *__restrict__ cell_cnt)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const StructGrid &g = grid[atom_struct[i]];
+    const double x[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    int cid = g.cell_base;
+    double y[3] = {x[0], x[1], x[2]};
+    if (g.pbc) {
+        int c[3];
+        double sh[3];
+        for (int n = 0; n < 3; ++n) {
+            const double f = g.B[3 * n] * x[0] + g.B[3 * n + 1] * x[1] + g.B[3 * n + 2] * x[2];
+            double k = floor(f);
+            double fw = f - k;
+            if (fw >= 1.0) { fw -= 1.0; k += 1.0; }
+            if (fw < 0.0) fw = 0.0;
+            sh[n] = k;
+            int cc = (int)(fw * g.nc[n]);
+            c[n] = cc >= g.nc[n] ? g.nc[n] - 1 : cc;
+        }
+        for (int d = 0; d < 3; ++d) y[d] = x[d] - (g.R[d] * sh[0] + g.R[3 + d] * sh[1] + g.R[6 + d] * sh[2]);
+        cid += (c[0] * g.nc[1] + c[1]) * g.nc[2] + c[2];
+    }
+    xw[3 * i] = y[0];
+    xw[3 * i + 1] = y[1];
+    xw[3 * i + 2] = y[2];
+    atom_cell[i] = cid;
+    atomicAdd(&cell_cnt[cid], 1);
+}
+
+// one block per structure: exclusive scan of its cells' counts
+__global__ void k_cell_start(const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
+                             const int *__restrict__ cell_cnt, int *__restrict__ cell_start, int *__restrict__ cell_fill,
+                             const int64_t *__restrict__ off)
+{
+    __shared__ int part[256];
+    const int s = blockIdx.x, t = threadIdx.x, T = blockDim.x;
+    const int base = grid[s].cell_base, nc = ncells[s];
+    const int chunk = (nc + T - 1) / T;
+    const int b = t * chunk, e = min(nc, b + chunk);
+    int sum = 0;
+    for (int k = b; k < e; ++k) sum += cell_cnt[base + k];
+    part[t] = sum;
+    __syncthreads();
+    for (int d = 1; d < T; d <<= 1) {
+        const int v = (t >= d) ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = (int)off[s] + part[t] - sum;
+    for (int k = b; k < e; ++k) {
+        cell_start[base + k] = run;
+        cell_fill[base + k] = 0;
+        run += cell_cnt[base + k];
+    }
+}
+
+__global__ void k_fill(int64_t N, const int *__restrict__ atom_cell, const int *__restrict__ cell_start,
+                       int *__restrict__ cell_fill, int *__restrict__ cell_atoms)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int c = atom_cell[i];
+    const int slot = cell_start[c] + atomicAdd(&cell_fill[c], 1);
+    cell_atoms[slot] = (int)i;
+}
+
+// one block per structure: insertion sort of every cell's member list, so the
+// neighbour order does not depend on the order of the atomic insertions
+__global__ void k_sort_cells(const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
+                             const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
+                             int *__restrict__ cell_atoms)
+{
+    const int s = blockIdx.x;
+    const int base = grid[s].cell_base, nc = ncells[s];
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+        int *a = cell_atoms + cell_start[base + k];
+        const int n = cell_cnt[base + k];
+        for (int p = 1; p < n; ++p) {
+            const int v = a[p];
+            int q = p - 1;
+            while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
+            a[q + 1] = v;
+        }
+    }
+}
+
+// one warp per atom.  Candidates are the members of the (2m+1)^3 cells around
+// the atom's cell, each with its lattice image shift; the FP64 displacement
+// x_i - (x_j + R q) decides membership (r^2 < rc^2; a self image needs
+// r^2 > 1e-12 as in neighbor.cpp:78).  The accepted list keeps candidate order
+// and is written grouped by neighbour type: float4(dx,dy,dz, j | type<<28).
+__global__ void __launch_bounds__(WARPS * 32) k_neigh(int64_t N, const int *__restrict__ atom_struct,
+                                                     const int *__restrict__ atom_cell, const StructGrid *__restrict__ grid,
+                                                     const double *__restrict__ xw, const int *__restrict__ type,
+                                                     const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
+                                                     const int *__restrict__ cell_atoms, double rc2, int cap, int ntypes,
+                                                     float4 *__restrict__ nbr, int *__restrict__ nbr_cnt, DevErr *err)
+{
+    __shared__ float4 s_lst[WARPS][NNP_MAX_NBR];
+    __shared__ int s_j[WARPS][NNP_MAX_NBR];
+    __shared__ unsigned char s_t[WARPS][NNP_MAX_NBR];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
+        const StructGrid &g = grid[atom_struct[i]];
+        const double xi0 = xw[3 * i], xi1 = xw[3 * i + 1], xi2 = xw[3 * i + 2];
+        const int local = atom_cell[i] - g.cell_base;
+        const int c2 = local % g.nc[2], c1 = (local / g.nc[2]) % g.nc[1], c0 = local / (g.nc[1] * g.nc[2]);
+        const int w0 = 2 * g.m[0] + 1, w1 = 2 * g.m[1] + 1, w2 = 2 * g.m[2] + 1;
+        const int O = w0 * w1 * w2;
+        int count = 0;
+        for (int ob = 0; ob < O; ob += 32) {
+            const int o = ob + lane;
+            int cnt = 0, start = 0, q0 = 0, q1 = 0, q2 = 0;
+            if (o < O) {
+                const int d2 = o % w2 - g.m[2];
+                const int t = o / w2;
+                const int d1 = t % w1 - g.m[1];
+                const int d0 = t / w1 - g.m[0];
+                const int t0 = c0 + d0, t1 = c1 + d1, t2 = c2 + d2;
+                q0 = floor_div(t0, g.nc[0]);
+                q1 = floor_div(t1, g.nc[1]);
+                q2 = floor_div(t2, g.nc[2]);
+                const int cw = g.cell_base + ((t0 - q0 * g.nc[0]) * g.nc[1] + (t1 - q1 * g.nc[1])) * g.nc[2] + (t2 - q2 * g.nc[2]);
+                cnt = cell_cnt[cw];
+                start = cell_start[cw];
+            }
+            int inc = cnt;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(FULL, inc, d);
+                if (lane >= d) inc += v;
+            }
+            const int exc = inc - cnt;
+            const int total = __shfl_sync(FULL, inc, 31);
+            for (int kb = 0; kb < total; kb += 32) {
+                const int k = kb + lane;
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step; step >>= 1) {
+                    const int ex = __shfl_sync(FULL, exc, lo + step);
+                    if (ex <= k) lo += step;
+                }
+                const int st = __shfl_sync(FULL, start, lo);
+                const int ex = __shfl_sync(FULL, exc, lo);
+                const double Q0 = __shfl_sync(FULL, q0, lo), Q1 = __shfl_sync(FULL, q1, lo), Q2 = __shfl_sync(FULL, q2, lo);
+                bool acc = false;
+                float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+                int j = 0;
+                if (k < total) {
+                    j = cell_atoms[st + k - ex];
+                    const double dx = xi0 - (xw[3 * (int64_t)j] + (g.R[0] * Q0 + g.R[3] * Q1 + g.R[6] * Q2));
+                    const double dy = xi1 - (xw[3 * (int64_t)j + 1] + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
+                    const double dz = xi2 - (xw[3 * (int64_t)j + 2] + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12)) {
+                        acc = true;
+                        e = make_float4((float)dx, (float)dy, (float)dz, 0.f);
+                    }
+                }
+                const unsigned bal = __ballot_sync(FULL, acc);
+                const int p = count + __popc(bal & lt);
+                if (acc && p < NNP_MAX_NBR) {
+                    s_lst[warp][p] = e;
+                    s_j[warp][p] = j;
+                    s_t[warp][p] = (unsigned char)type[j];
+                }
+                count += __popc(bal);
+            }
+        }
+        __syncwarp();
+        const int nw = min(count, NNP_MAX_NBR);
+        if (count > cap && lane == 0) atomicMax(&err->need_cap, count);
+        int outp = 0;
+        for (int t = 0; t < ntypes; ++t) {
+            for (int kb = 0; kb < nw; kb += 32) {
+                const int k = kb + lane;
+                const bool m = (k < nw) && s_t[warp][k] == t;
+                const unsigned bal = __ballot_sync(FULL, m);
+                const int p = outp + __popc(bal & lt);
+                if (m && p < cap) {
+                    float4 e = s_lst[warp][k];
+                    e.w = __int_as_float(s_j[warp][k] | (t << 28));
+                    nbr[i * cap + p] = e;
+                }
+                outp += __popc(bal);
+            }
+        }
+        if (lane == 0) nbr_cnt[i] = min(count, cap);
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ per-atom staging
+
+// Per-warp shared-memory view of one atom's neighbours (structure of arrays).
+struct NbrView {
+    float *ux, *uy, *uz, *r;
+    int *j;
+    unsigned char *t;
+    float *fc, *fd;     // [ncut][C]
+    float *w, *wd;      // [ndamp][C]
+    float *gx, *gy, *gz;
+    float4 *par;        // block parameters [NNP_MAX_AFUNC]
+    float *vec;         // G or dE/dG row [gstride]
+    int *seg;           // [NNP_MAX_TYPES+1] segment starts
+};
+
+__host__ __device__ inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride)
+{
+    // ux uy uz r j(t packed as bytes) fc fd w wd gx gy gz, params, vec, seg
+    return C * (4 + 1 + 2 * ncut + 2 * ndamp + 3) + (C + 3) / 4 + 4 * NNP_MAX_AFUNC + gstride + NNP_MAX_TYPES + 1;
+}
+
+__device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride)
+{
+    NbrView v;
+    float *p = base;
+    v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;   // 16-byte aligned first
+    v.ux = p; p += C;
+    v.uy = p; p += C;
+    v.uz = p; p += C;
+    v.r = p; p += C;
+    v.j = reinterpret_cast<int *>(p); p += C;
+    v.fc = p; p += ncut * C;
+    v.fd = p; p += ncut * C;
+    v.w = p; p += ndamp * C;
+    v.wd = p; p += ndamp * C;
+    v.gx = p; p += C;
+    v.gy = p; p += C;
+    v.gz = p; p += C;
+    v.vec = p; p += gstride;
+    v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
+    v.t = reinterpret_cast<unsigned char *>(p);
+    return v;
+}
+
+// Load atom i's neighbour list into the warp's view and compute the per-neighbour
+// quantities: unit vector, distance, cutoff value/slope per cutoff, and the
+// GAUSS damping factors w_e(r) = fc(r) exp(-a_e r^2) with slopes dw_e/dr.
+__device__ inline int stage_neighbors(const NbrView &v, int64_t i, int cap, const float4 *__restrict__ nbr,
+                                      const int *__restrict__ nbr_cnt, const DevPot &P, const DevType &T, int lane)
+{
+    const int n = nbr_cnt[i];
+    for (int k = lane; k < n; k += 32) {
+        const float4 e = nbr[i * cap + k];
+        const float r = sqrtf(e.x * e.x + e.y * e.y + e.z * e.z);
+        const float ir = 1.f / r;
+        v.ux[k] = e.x * ir;
+        v.uy[k] = e.y * ir;
+        v.uz[k] = e.z * ir;
+        v.r[k] = r;
+        const int pk = __float_as_int(e.w);
+        v.j[k] = pk & 0x0fffffff;
+        v.t[k] = (unsigned char)((unsigned)pk >> 28);
+        for (int c = 0; c < P.ncut; ++c) {
+            float f, g;
+            cutoff_fg(P.cut[c], r, f, g);
+            v.fc[c * cap + k] = f;
+            v.fd[c * cap + k] = g;
+        }
+        for (int d = 0; d < T.ndamp; ++d) {
+            const int c = T.damp_cut[d];
+            const float a = T.damp_a[d];
+            const float ex = expf(-a * r * r);
+            const float f = v.fc[c * cap + k], g = v.fd[c * cap + k];
+            v.w[d * cap + k] = f * ex;
+            v.wd[d * cap + k] = (g - 2.f * a * r * f) * ex;
+        }
+    }
+    // type segment starts (list is grouped by type)
+    for (int t = 0; t <= P.ntypes; ++t) {
+        int c = 0;
+        for (int kb = 0; kb < n; kb += 32) {
+            const int k = kb + lane;
+            c += __popc(__ballot_sync(FULL, k < n && v.t[k] < t));
+        }
+        if (lane == 0) v.seg[t] = c;
+    }
+    __syncwarp();
+    return n;
+}
+
+// first (a,b) of a lane in a block's pair list and the advance by 32:
+// rectangle rows x cols (J != K) or lower triangle a > b of one segment (J == K)
+struct PairIter {
+    int a, b;
+};
+
+__device__ __forceinline__ void pair_first(bool tri, int cols, int lane, PairIter &p)
+{
+    if (tri) {
+        p.a = 1;
+        p.b = lane;
+        while (p.b >= p.a) { p.b -= p.a; ++p.a; }
+    } else {
+        p.a = lane / cols;
+        p.b = lane - p.a * cols;
+    }
+}
+
+__device__ __forceinline__ void pair_next(bool tri, int cols, PairIter &p)
+{
+    p.b += 32;
+    if (tri) {
+        while (p.b >= p.a) { p.b -= p.a; ++p.a; }
+    } else {
+        while (p.b >= cols) { p.b -= cols; ++p.a; }
+    }
+}
+
+__device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
+{
+    K = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
+    while (K * (K + 1) / 2 > tt) --K;
+    while ((K + 1) * (K + 2) / 2 <= tt) ++K;
+    J = tt - K * (K + 1) / 2;
+}
+
+// ------------------------------------------------------------------ symmetry functions
+
+__global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot *__restrict__ pot,
+                                                    const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
+                                                    const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                    const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
+                                                    int gstride, float *__restrict__ G)
+{
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride);
+    const DevPot &P = *pot;
+    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
+        const int II = type[i];
+        const DevType &T = P.t[II];
+        stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        float *Gi = G + i * gstride;
+        for (int g = lane; g < gstride; g += 32) Gi[g] = 0.f;
+        __syncwarp();
+        // ---- radial: one block per neighbour type; lanes own functions and
+        // walk that type's neighbour segment (no cross-lane reduction)
+        for (int J = 0; J < P.ntypes; ++J) {
+            const DevBlockR B = T.br[J];
+            if (B.n == 0) continue;
+            const int s0 = v.seg[J], s1 = v.seg[J + 1];
+            for (int f = lane; f < B.n; f += 32) {
+                const float2 q = rpar[B.par + f];
+                float acc = 0.f;
+                for (int k = s0; k < s1; ++k) {
+                    float val, der;
+                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
+                    acc += val;
+                }
+                Gi[B.off_g + f] = acc;
+            }
+        }
+        // ---- angular: one block per neighbour-type pair J <= K
+        const int TT = P.ntypes * (P.ntypes + 1) / 2;
+        for (int tt = 0; tt < TT; ++tt) {
+            const DevBlockA B = T.ba[tt];
+            if (B.n == 0) continue;
+            int J, K;
+            tt_decode(tt, J, K);
+            const int sa = v.seg[J], na = v.seg[J + 1] - sa;
+            const int sb = v.seg[K], nb = v.seg[K + 1] - sb;
+            const bool tri = (J == K);
+            const int npairs = tri ? na * (na - 1) / 2 : na * nb;
+            if (npairs == 0) continue;
+            for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
+            __syncwarp();
+            if (B.form == ANG_GAUSS) {
+                // GAUSS: damping exp(-(ra^2+rb^2)/eta^2) fc(ra) fc(rb) = w(ra) w(rb)
+                // from the staged per-neighbour factors; functions in chunks of
+                // SYMM_CHUNK register accumulators
+                for (int f0 = 0; f0 < B.n; f0 += SYMM_CHUNK) {
+                    const int nf = min(SYMM_CHUNK, B.n - f0);
+                    float acc[SYMM_CHUNK];
+#pragma unroll
+                    for (int f = 0; f < SYMM_CHUNK; ++f) acc[f] = 0.f;
+                    PairIter it;
+                    pair_first(tri, nb, lane, it);
+                    for (int p = lane; p < npairs; p += 32) {
+                        const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
+                        const float cs = v.ux[a] * v.ux[b] + v.uy[a] * v.uy[b] + v.uz[a] * v.uz[b];
+                        int dcur = -1;
+                        float damp = 0.f;
+#pragma unroll
+                        for (int f = 0; f < SYMM_CHUNK; ++f) {
+                            if (f < nf) {
+                                const float4 q = v.par[f0 + f];
+                                const int pk = __float_as_int(q.w);
+                                const int d = pk & 0xff, iz = (pk >> 8) - 1;
+                                if (d != dcur) {
+                                    dcur = d;
+                                    damp = v.w[d * cap + a] * v.w[d * cap + b];
+                                }
+                                const float x = fabsf(0.5f + q.x * cs);
+                                acc[f] += zpow(x, q.y, iz) * damp;
+                            }
+                        }
+                        pair_next(tri, nb, it);
+                    }
+#pragma unroll
+                    for (int f = 0; f < SYMM_CHUNK; ++f) {
+                        if (f < nf) {
+                            const float s = warp_sum(acc[f]);
+                            if (lane == 0) Gi[B.off_g + f0 + f] = s;
+                        }
+                    }
+                }
+            } else {
+                // other forms: one function per pass over the pairs
+                for (int f = 0; f < B.n; ++f) {
+                    const float4 q = v.par[f];
+                    const int iz = (__float_as_int(q.w) >> 8) - 1;
+                    float acc = 0.f;
+                    PairIter it;
+                    pair_first(tri, nb, lane, it);
+                    for (int p = lane; p < npairs; p += 32) {
+                        const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
+                        const float cs = v.ux[a] * v.ux[b] + v.uy[a] * v.uy[b] + v.uz[a] * v.uz[b];
+                        float h, hc, hrj, hrk;
+                        angular_generic(B.form, v.r[a], v.r[b], cs, v.fc[B.cut * cap + a], v.fc[B.cut * cap + b], 0.f,
+                                        0.f, q.x, q.y, iz, q.z, false, h, hc, hrj, hrk);
+                        acc += h;
+                        pair_next(tri, nb, it);
+                    }
+                    acc = warp_sum(acc);
+                    if (lane == 0) Gi[B.off_g + f] = acc;
+                }
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ networks (FP32)
+
+// Network of type t in shared memory, layout of nnp_internal.h (net_floats).
+struct NetView {
+    const float *inpw, *inpb, *outw, *outb;
+    const float *b[NNP_MAX_LAYERS];
+    const float *wt[NNP_MAX_LAYERS];
+    int ws[NNP_MAX_LAYERS];   // row stride of W^T
+};
+
+__device__ inline NetView net_view(const float *base, const DevType &T)
+{
+    NetView v;
+    const float *p = base;
+    const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+    v.inpw = p; p += nin;
+    v.inpb = p; p += nin;
+    v.outw = p; p += nout;
+    v.outb = p; p += nout;
+    for (int l = 0; l < T.nlayer; ++l) {
+        const int ni = T.nodes[l], no = T.nodes[l + 1];
+        v.b[l] = p; p += no;
+        v.ws[l] = wt_stride(no);
+        v.wt[l] = p; p += (int64_t)ni * v.ws[l];
+    }
+    return v;
+}
+
+// One warp per atom: forward pass, atomic energy, and the input gradient
+// dE/dG = outw d_L W_L ... d_0 W_0 diag(inpw) (DODZ::grad).
+__global__ void __launch_bounds__(WARPS * 32) k_nn_fp32(int64_t N, const DevPot *__restrict__ pot,
+                                                       const float *__restrict__ wpar, int64_t wfloats,
+                                                       const int *__restrict__ type, const float *__restrict__ G,
+                                                       int gstride, int maxn, float *__restrict__ e_atom,
+                                                       float *__restrict__ dEdG)
+{
+    extern __shared__ float smem[];
+    float *w_s = smem;
+    for (int64_t k = threadIdx.x; k < wfloats; k += blockDim.x) w_s[k] = wpar[k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *ws = smem + ((wfloats + 3) & ~3) + (size_t)warp * (NNP_MAX_LAYERS + 2) * maxn;
+    float *xa = ws;                      // activations (ping)
+    float *xb = ws + maxn;               // activations (pong)
+    float *dd = ws + 2 * maxn;           // f'(z) per layer [nlayer][maxn]
+    const DevPot &P = *pot;
+    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
+        const DevType &T = P.t[type[i]];
+        const NetView V = net_view(w_s + T.woff, T);
+        const int L = T.nlayer, nin = T.nodes[0];
+        const float *Gi = G + i * gstride;
+        for (int m = lane; m < nin; m += 32) xa[m] = V.inpw[m] * (Gi[m] + V.inpb[m]);
+        __syncwarp();
+        float *x = xa, *y = xb;
+        for (int l = 0; l < L; ++l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], s = V.ws[l];
+            const int neu = (l == L - 1) ? NEU_LINEAR : T.neuron;
+            for (int n = lane; n < no; n += 32) {
+                float z = V.b[l][n];
+                const float *wc = V.wt[l] + n;
+                for (int m = 0; m < ni; ++m) z += wc[m * s] * x[m];
+                float a, d, d2;
+                activation(neu, T.c, z, a, d, d2);
+                y[n] = a;
+                dd[l * maxn + n] = d;
+            }
+            __syncwarp();
+            float *tmp = x; x = y; y = tmp;
+        }
+        if (lane == 0) e_atom[i] = V.outb[0] + x[0] * V.outw[0];
+        // backward: delta_L = outw * d_L, delta_{l-1} = (W_l^T delta_l) * d_{l-1}
+        if (lane == 0) y[0] = V.outw[0] * dd[(L - 1) * maxn];
+        __syncwarp();
+        float *dl = y, *dn = x;
+        for (int l = L - 1; l >= 1; --l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], s = V.ws[l];
+            for (int m = lane; m < ni; m += 32) {
+                const float *wr = V.wt[l] + m * s;
+                float t = 0.f;
+                for (int n = 0; n < no; ++n) t += wr[n] * dl[n];
+                dn[m] = t * dd[(l - 1) * maxn + m];
+            }
+            __syncwarp();
+            float *tmp = dl; dl = dn; dn = tmp;
+        }
+        {
+            const int no = T.nodes[1], s = V.ws[0];
+            float *out = dEdG + i * gstride;
+            for (int m = lane; m < nin; m += 32) {
+                const float *wr = V.wt[0] + m * s;
+                float t = 0.f;
+                for (int n = 0; n < no; ++n) t += wr[n] * dl[n];
+                out[m] = t * V.inpw[m];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ forces
+
+// One warp per atom.  With e = dE_i/dG_i, every pair and triplet contributes
+// dE_i/dd_j for the neighbour displacements d_j = x_i - x_j - R q; the warp
+// accumulates g_j = dE_i/dd_j per neighbour slot, then F_j += g_j and
+// F_i -= sum_j g_j (FP64 atomics) -- the same Newton-3 scatter as
+// nnp.cpp:443-471.
+__global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot *__restrict__ pot,
+                                                     const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
+                                                     const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                     const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
+                                                     int gstride, const float *__restrict__ dEdG,
+                                                     double *__restrict__ F, DevErr *err)
+{
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride);
+    const DevPot &P = *pot;
+    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
+        const int II = type[i];
+        const DevType &T = P.t[II];
+        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        const float *e = dEdG + i * gstride;
+        for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
+        __syncwarp();
+        // ---- radial: lanes own their neighbour slot
+        for (int k = lane; k < n; k += 32) {
+            const DevBlockR B = T.br[v.t[k]];
+            const float r = v.r[k];
+            const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
+            float amp = 0.f;
+            for (int f = 0; f < B.n; ++f) {
+                const float2 q = rpar[B.par + f];
+                float val, der;
+                radial_fd(B.form, r, q.x, q.y, fc, fd, val, der);
+                amp += v.vec[B.off_g + f] * der;
+            }
+            v.gx[k] = amp * v.ux[k];
+            v.gy[k] = amp * v.uy[k];
+            v.gz[k] = amp * v.uz[k];
+        }
+        __syncwarp();
+        // ---- angular
+        const int TT = P.ntypes * (P.ntypes + 1) / 2;
+        for (int tt = 0; tt < TT; ++tt) {
+            const DevBlockA B = T.ba[tt];
+            if (B.n == 0) continue;
+            int J, K;
+            tt_decode(tt, J, K);
+            const int sa = v.seg[J], na = v.seg[J + 1] - sa;
+            const int sb = v.seg[K], nb = v.seg[K + 1] - sb;
+            const bool tri = (J == K);
+            const int npairs = tri ? na * (na - 1) / 2 : na * nb;
+            if (npairs == 0) continue;
+            for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
+            __syncwarp();
+            const float *eb = v.vec + B.off_g;
+            const bool gauss = (B.form == ANG_GAUSS);
+            PairIter it;
+            pair_first(tri, nb, lane, it);
+            for (int p = lane; p < npairs; p += 32) {
+                const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
+                const float uax = v.ux[a], uay = v.uy[a], uaz = v.uz[a];
+                const float ubx = v.ux[b], uby = v.uy[b], ubz = v.uz[b];
+                const float cs = uax * ubx + uay * uby + uaz * ubz;
+                float hc = 0.f, hra = 0.f, hrb = 0.f;   // dE/dcos, dE/dr_a, dE/dr_b
+                if (gauss) {
+                    int dcur = -1;
+                    float sc = 0.f, sp = 0.f;
+#pragma unroll 2
+                    for (int f = 0; f < B.n; ++f) {
+                        {
+                            const float4 q = v.par[f];
+                            const int pk = __float_as_int(q.w);
+                            const int d = pk & 0xff, iz = (pk >> 8) - 1;
+                            if (d != dcur) {
+                                if (dcur >= 0) {
+                                    const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                                    hc += sc * wa * wb;
+                                    hra += sp * v.wd[dcur * cap + a] * wb;
+                                    hrb += sp * wa * v.wd[dcur * cap + b];
+                                }
+                                dcur = d;
+                                sc = 0.f;
+                                sp = 0.f;
+                            }
+                            const float x = fabsf(0.5f + q.x * cs);
+                            const float pm1 = (iz > 0) ? ipow(x, iz - 1) : ((iz == 0) ? 0.f : zpow(x, q.y - 1.f, -1));
+                            const float pz = (iz == 0) ? 1.f : pm1 * x;
+                            const float ef = eb[f];
+                            sc += ef * q.y * q.x * pm1;
+                            sp += ef * pz;
+                        }
+                    }
+                    if (dcur >= 0) {
+                        const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                        hc += sc * wa * wb;
+                        hra += sp * v.wd[dcur * cap + a] * wb;
+                        hrb += sp * wa * v.wd[dcur * cap + b];
+                    }
+                } else {
+                    const float ra = v.r[a], rb = v.r[b];
+                    const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];
+                    const float ga = v.fd[B.cut * cap + a], gb = v.fd[B.cut * cap + b];
+#pragma unroll 1
+                    for (int f = 0; f < B.n; ++f) {
+                        {
+                            const float4 q = v.par[f];
+                            const int iz = (__float_as_int(q.w) >> 8) - 1;
+                            float h, dc, dra, drb;
+                            angular_generic(B.form, ra, rb, cs, ca, cb, ga, gb, q.x, q.y, iz, q.z, true, h, dc, dra, drb);
+                            const float ef = eb[f];
+                            hc += ef * dc;
+                            hra += ef * dra;
+                            hrb += ef * drb;
+                        }
+                    }
+                }
+                const float ira = 1.f / v.r[a], irb = 1.f / v.r[b];
+                const float ca_ = hra - hc * cs * ira, cb_ = hc * ira;
+                atomicAdd(&v.gx[a], ca_ * uax + cb_ * ubx);
+                atomicAdd(&v.gy[a], ca_ * uay + cb_ * uby);
+                atomicAdd(&v.gz[a], ca_ * uaz + cb_ * ubz);
+                const float cc_ = hrb - hc * cs * irb, cd_ = hc * irb;
+                atomicAdd(&v.gx[b], cc_ * ubx + cd_ * uax);
+                atomicAdd(&v.gy[b], cc_ * uby + cd_ * uay);
+                atomicAdd(&v.gz[b], cc_ * ubz + cd_ * uaz);
+                pair_next(tri, nb, it);
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+        // ---- scatter: F_j += g_j, F_i -= sum g_j
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        bool bad = false;
+        for (int k = lane; k < n; k += 32) {
+            const float gx = v.gx[k], gy = v.gy[k], gz = v.gz[k];
+            bad |= !(isfinite(gx) && isfinite(gy) && isfinite(gz));
+            const int64_t j = v.j[k];
+            atomicAdd(&F[3 * j], (double)gx);
+            atomicAdd(&F[3 * j + 1], (double)gy);
+            atomicAdd(&F[3 * j + 2], (double)gz);
+            fx += gx;
+            fy += gy;
+            fz += gz;
+        }
+        fx = warp_sum_d(fx);
+        fy = warp_sum_d(fy);
+        fz = warp_sum_d(fz);
+        if (lane == 0) {
+            atomicAdd(&F[3 * i], -fx);
+            atomicAdd(&F[3 * i + 1], -fy);
+            atomicAdd(&F[3 * i + 2], -fz);
+        }
+        if (__any_sync(FULL, bad) && lane == 0) atomicMax(&err->nonfinite, 1);
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ energies
+
+__global__ void k_energy(const int64_t *__restrict__ off, const float *__restrict__ e_atom,
+                         const int *__restrict__ type, const DevPot *__restrict__ pot, int vacuum,
+                         const double *__restrict__ vac, double *__restrict__ e_struct, DevErr *err)
+{
+    __shared__ double part[256];
+    const int s = blockIdx.x;
+    double sum = 0.0;
+    for (int64_t a = off[s] + threadIdx.x; a < off[s + 1]; a += blockDim.x) {
+        sum += (double)e_atom[a];
+        if (vacuum) sum += vac[type[a]];
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int d = blockDim.x / 2; d; d >>= 1) {
+        if (threadIdx.x < d) part[threadIdx.x] += part[threadIdx.x + d];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        e_struct[s] = part[0];
+        if (!isfinite(part[0])) atomicMax(&err->nonfinite, 1);
+    }
+}
+
+__global__ void k_f2d(int64_t n, const float *__restrict__ a, double *__restrict__ b)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+
+__global__ void k_d2f(int64_t n, const double *__restrict__ a, float *__restrict__ b)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+// ------------------------------------------------------------------ host launch sequence
+
+static int num_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+static int ncut_max(const Engine &E) { return E.dpot.ncut > 0 ? E.dpot.ncut : 1; }
+
+static int ndamp_max(const Engine &E)
+{
+    int m = 1;
+    for (int t = 0; t < E.dpot.ntypes; ++t) m = std::max(m, E.dpot.t[t].ndamp);
+    return m;
+}
+
+static size_t view_bytes(const Engine &E)
+{
+    const int per = nbr_view_floats(E.cap, ncut_max(E), ndamp_max(E), E.gstride);
+    return (size_t)WARPS * ((per + 3) & ~3) * sizeof(float);
+}
+
+std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
+{
+    (void)pbc;
+    E.n_atoms = n_atoms;
+    E.n_struct = n_struct;
+    const size_t N = (size_t)std::max<int64_t>(n_atoms, 1), S = (size_t)std::max(n_struct, 1);
+    const size_t cell_bound = 64 * S + 2 * N + 64;
+    cudaError_t e = cudaSuccess;
+    auto r = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
+    r(E.xw.reserve(3 * N));
+    r(E.atom_struct.reserve(N));
+    r(E.atom_cell.reserve(N));
+    r(E.grid.reserve(S));
+    r(E.scan_tmp.reserve(S));
+    r(E.cell_cnt.reserve(cell_bound));
+    r(E.cell_start.reserve(cell_bound));
+    r(E.cell_fill.reserve(cell_bound));
+    r(E.cell_atoms.reserve(N));
+    r(E.nbr.reserve(N * (size_t)E.cap));
+    r(E.nbr_cnt.reserve(N));
+    r(E.G.reserve(N * (size_t)E.gstride));
+    r(E.dEdG.reserve(N * (size_t)E.gstride));
+    r(E.e_atom.reserve(N));
+    r(E.e_struct.reserve(S));
+    r(E.force.reserve(3 * N));
+    r(E.err.reserve(1));
+    if (e != cudaSuccess) return std::string("device allocation failed: ") + cudaGetErrorString(e);
+    cudaMemsetAsync(E.err.p, 0, sizeof(DevErr), E.stream);
+    return cuda_msg("prepare");
+}
+
+std::string run_neighbors(Engine &E, int pbc)
+{
+    const int64_t N = E.n_atoms;
+    const int S = E.n_struct;
+    if (N == 0 || S == 0) return "";
+    cudaStream_t st = E.stream;
+    k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
+                                                             E.dpot.ntypes, E.err.p);
+    k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
+                                                              E.grid.p, E.scan_tmp.p, E.err.p);
+    k_cell_base<<<1, 1024, 0, st>>>(E.scan_tmp.p, S, E.grid.p);
+    const size_t cell_bound = 64 * (size_t)S + 2 * (size_t)N + 64;
+    cudaMemsetAsync(E.cell_cnt.p, 0, cell_bound * sizeof(int), st);
+    k_bin<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.pos.p, E.atom_struct.p, E.grid.p, E.xw.p, E.atom_cell.p,
+                                                     E.cell_cnt.p);
+    k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
+    k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
+    k_sort_cells<<<S, 128, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p);
+    const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
+    k_neigh<<<grid_for(N, WARPS, num_sms() * 8), WARPS * 32, 0, st>>>(
+        N, E.atom_struct.p, E.atom_cell.p, E.grid.p, E.xw.p, E.type.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p,
+        rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
+    return cuda_msg("neighbour list");
+}
+
+std::string run_symm(Engine &E)
+{
+    const int64_t N = E.n_atoms;
+    if (N == 0) return "";
+    const size_t sm = view_bytes(E);
+    cudaFuncSetAttribute(k_symm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_symm<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
+        N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
+        E.G.p);
+    return cuda_msg("symmetry functions");
+}
+
+static int max_nodes(const Engine &E)
+{
+    int m = 1;
+    for (int t = 0; t < E.dpot.ntypes; ++t)
+        for (int l = 0; l <= E.dpot.t[t].nlayer; ++l) m = std::max(m, E.dpot.t[t].nodes[l]);
+    return (m + 3) & ~3;
+}
+
+std::string run_nn(Engine &E)
+{
+    const int64_t N = E.n_atoms;
+    if (N == 0) return "";
+    const int maxn = max_nodes(E);
+    const size_t sm = (size_t)(((E.wfloats + 3) & ~3) + WARPS * (NNP_MAX_LAYERS + 2) * maxn) * sizeof(float);
+    if (sm > 220 * 1024) return "networks too large for the shared-memory FP32 path";
+    cudaFuncSetAttribute(k_nn_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_nn_fp32<<<grid_for(N, WARPS * 8, num_sms() * 2), WARPS * 32, sm, E.stream>>>(
+        N, E.d_pot, E.wpar.p, E.wfloats, E.type.p, E.G.p, E.gstride, maxn, E.e_atom.p, E.dEdG.p);
+    return cuda_msg("networks");
+}
+
+std::string run_force(Engine &E)
+{
+    const int64_t N = E.n_atoms;
+    if (N == 0) return "";
+    cudaMemsetAsync(E.force.p, 0, 3 * (size_t)N * sizeof(double), E.stream);
+    const size_t sm = view_bytes(E);
+    cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_force<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
+        N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
+        E.dEdG.p, E.force.p, E.err.p);
+    return cuda_msg("forces");
+}
+
+std::string run_energy(Engine &E, bool vacuum)
+{
+    if (E.n_struct == 0) return "";
+    k_energy<<<E.n_struct, 256, 0, E.stream>>>(E.atom_off.p, E.e_atom.p, E.type.p, E.d_pot, vacuum ? 1 : 0,
+                                               E.vac.p, E.e_struct.p, E.err.p);
+    return cuda_msg("energies");
+}
+
+std::string run_symm_to_double(Engine &E, double *out)
+{
+    const int64_t n = E.n_atoms * E.gstride;
+    if (n == 0) return "";
+    k_f2d<<<grid_for(n, 256, 1 << 30), 256, 0, E.stream>>>(n, E.G.p, out);
+    return cuda_msg("symm copy");
+}
+
+std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in)
+{
+    (void)gstride_in;
+    const int64_t n = E.n_atoms * E.gstride;
+    if (n == 0) return "";
+    k_d2f<<<grid_for(n, 256, 1 << 30), 256, 0, E.stream>>>(n, symm_d, E.G.p);
+    return run_nn(E);
+}
+
+}  // namespace nnp

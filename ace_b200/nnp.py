@@ -1,0 +1,254 @@
+"""Python front end of libnnp_b200.so (the C ABI in include/nnp_b200.h).
+
+``NNP`` keeps the method names of the reference's ``NNP`` class
+(src/nnp/nnp.hpp:64-121): ``read``, ``write``, ``compute_symm``,
+``compute_energy``, ``compute_force``, ``compute``, ``index``, ``ntypes``,
+``rc``.  Errors raise ``NNPError`` (the reference throws
+``std::invalid_argument`` / ``std::runtime_error``).  The library is loaded
+from this package directory; there is no fallback when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libnnp_b200.so")
+
+NNP_OK = 0
+ERRORS = {-1: "ARG", -2: "IO", -3: "PARSE", -4: "CUDA", -5: "CAPACITY", -6: "UNSUPPORTED", -7: "TYPE",
+          -8: "NOT_FINITE"}
+PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
+ENERGY, FORCES, VACUUM, DEVICE_PTRS, SYMM = 1, 2, 4, 8, 16
+
+
+class NNPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s (%s)" % (msg, ERRORS.get(code, code)))
+        self.code = code
+
+
+class _Batch(C.Structure):
+    _fields_ = [("n_struct", C.c_int32), ("atom_off", C.c_void_p), ("pos", C.c_void_p), ("type", C.c_void_p),
+                ("cell", C.c_void_p), ("pbc", C.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise ImportError("libnnp_b200.so is not built (run make -C ace_b200 or __graft_entry__.build())")
+        L = C.CDLL(LIBPATH)
+        p, i, d, u = C.c_void_p, C.c_int32, C.c_double, C.c_uint32
+        sig = {
+            "nnp_create_from_file": ([C.c_char_p, C.POINTER(p)], i),
+            "nnp_create_from_basis": ([i, p, d, p, p, C.POINTER(p)], i),
+            "nnp_destroy": ([p], i),
+            "nnp_write": ([p, C.c_char_p], i),
+            "nnp_set_precision": ([p, i], i),
+            "nnp_set_stream": ([p, p], i),
+            "nnp_ntypes": ([p, C.POINTER(i)], i),
+            "nnp_type_index": ([p, C.c_char_p, C.POINTER(i)], i),
+            "nnp_rc": ([p, C.POINTER(d)], i),
+            "nnp_n_input": ([p, i, C.POINTER(i)], i),
+            "nnp_compute": ([p, C.POINTER(_Batch), p, p, p, u], i),
+            "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
+            "nnp_nparams": ([p, i, C.POINTER(i)], i),
+            "nnp_get_params": ([p, p], i),
+            "nnp_set_params": ([p, p], i),
+            "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
+            "nnp_last_error": ([p], C.c_char_p),
+            "nnp_version": ([], C.c_char_p),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class NNP:
+    """A potential resident on the GPU (one C-ABI handle)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    # ---- construction: NNP::read (nnp.cpp:181-190)
+    @classmethod
+    def read(cls, path: str) -> "NNP":
+        h = C.c_void_p()
+        rc = lib().nnp_create_from_file(os.fsencode(path), C.byref(h))
+        if rc != NNP_OK:
+            raise NNPError(rc, lib().nnp_last_error(None).decode())
+        return cls(h)
+
+    @classmethod
+    def from_basis(cls, type_lines: Sequence[str], rc: float, basis_paths: Sequence[str],
+                   network_texts: Sequence[str]) -> "NNP":
+        """NNP::read_basis per element + a network per element (nnptefr.cpp:2023-2031)."""
+        n = len(type_lines)
+        tl = (C.c_char_p * n)(*[s.encode() for s in type_lines])
+        bp = (C.c_char_p * n)(*[os.fsencode(s) for s in basis_paths])
+        nt = (C.c_char_p * n)(*[s.encode() for s in network_texts])
+        h = C.c_void_p()
+        r = lib().nnp_create_from_basis(n, C.cast(tl, C.c_void_p), float(rc), C.cast(bp, C.c_void_p),
+                                        C.cast(nt, C.c_void_p), C.byref(h))
+        if r != NNP_OK:
+            raise NNPError(r, lib().nnp_last_error(None).decode())
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            lib().nnp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != NNP_OK:
+            raise NNPError(rc, lib().nnp_last_error(self._h).decode())
+
+    # ---- NNP::write (nnp.cpp:165-174)
+    def write(self, path: str):
+        self._check(lib().nnp_write(self._h, os.fsencode(path)))
+
+    # ---- access (nnp.hpp:78-87)
+    @property
+    def ntypes(self) -> int:
+        v = C.c_int32()
+        self._check(lib().nnp_ntypes(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def rc(self) -> float:
+        v = C.c_double()
+        self._check(lib().nnp_rc(self._h, C.byref(v)))
+        return v.value
+
+    def index(self, name: str) -> int:
+        v = C.c_int32()
+        self._check(lib().nnp_type_index(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def n_input(self, t: int) -> int:
+        v = C.c_int32()
+        self._check(lib().nnp_n_input(self._h, t, C.byref(v)))
+        return v.value
+
+    @property
+    def gstride(self) -> int:
+        g = max(self.n_input(t) for t in range(self.ntypes))
+        return (g + 3) & ~3
+
+    def set_precision(self, prec: int):
+        self._check(lib().nnp_set_precision(self._h, prec))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(lib().nnp_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def nparams(self, t: int = -1) -> int:
+        v = C.c_int32()
+        self._check(lib().nnp_nparams(self._h, t, C.byref(v)))
+        return v.value
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.nparams())
+        self._check(lib().nnp_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        if p.size != self.nparams():
+            raise NNPError(-1, "Invalid size: vector and network mismatch.")
+        self._check(lib().nnp_set_params(self._h, _ptr(p)))
+
+    # ---- batched compute
+    def compute_batch(self, atom_off, pos, types, cells, pbc=True, energy=True, forces=True,
+                      symm=False, vacuum=False):
+        """Energies [n_struct], forces [N,3] (and symmetry functions [N,gstride]) of a CSR batch."""
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        S = len(atom_off) - 1
+        cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(S, 9) if pbc else None
+        N = int(atom_off[-1]) if S else 0
+        b = _Batch(S, atom_off.ctypes.data, pos.ctypes.data, types.ctypes.data,
+                   cells.ctypes.data if cells is not None else None, 1 if pbc else 0)
+        E = np.zeros(max(S, 1))
+        F = np.zeros((max(N, 1), 3))
+        gs = self.gstride
+        G = np.zeros((max(N, 1), gs)) if symm else None
+        flags = (ENERGY if energy else 0) | (FORCES if forces else 0) | (SYMM if symm else 0) | (VACUUM if vacuum else 0)
+        self._check(lib().nnp_compute(self._h, C.byref(b), _ptr(E), _ptr(F), _ptr(G), flags))
+        out = [E[:S], F[:N]]
+        if symm:
+            out.append(G[:N])
+        return tuple(out)
+
+    def compute_device(self, atom_off_ptr: int, pos_ptr: int, type_ptr: int, cell_ptr: int, n_struct: int,
+                       energy_ptr: int, force_ptr: int, pbc: bool = True, vacuum: bool = False):
+        """Same as compute_batch on device-resident arrays (raw CUDA pointers)."""
+        b = _Batch(n_struct, atom_off_ptr, pos_ptr, type_ptr, cell_ptr, 1 if pbc else 0)
+        flags = ENERGY | FORCES | DEVICE_PTRS | (VACUUM if vacuum else 0)
+        self._check(lib().nnp_compute(self._h, C.byref(b), C.c_void_p(energy_ptr), C.c_void_p(force_ptr), None,
+                                      flags))
+
+    # ---- per-structure calls with the reference's names and semantics
+    def compute_symm(self, pos, types, cell, pbc=True) -> np.ndarray:
+        """NNP::compute_symm (nnp.cpp:350-398): symmetry functions, one row per atom."""
+        n = len(types)
+        _, _, G = self.compute_batch([0, n], pos, types, cell, pbc, energy=False, forces=False, symm=True)
+        return G
+
+    def compute_energy(self, types, symm) -> float:
+        """NNP::compute_energy (nnp.cpp:329-338): sum of network(G) + vacuum energies."""
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        symm = np.ascontiguousarray(symm, dtype=np.float64)
+        off = np.array([0, len(types)], dtype=np.int64)
+        E = np.zeros(1)
+        self._check(lib().nnp_compute_energy_symm(self._h, 1, _ptr(off), _ptr(types), _ptr(symm), symm.shape[1],
+                                                  _ptr(E)))
+        return float(E[0])
+
+    def compute_force(self, pos, types, cell, pbc=True):
+        """NNP::compute_force (nnp.cpp:412-482): (energy without vacuum terms, forces)."""
+        n = len(types)
+        E, F = self.compute_batch([0, n], pos, types, cell, pbc)
+        return float(E[0]), F
+
+    compute = compute_force   # NNP::compute (nnp.cpp:489-494) = build + symm + force
+
+    def train_grad(self, atom_off, pos, types, cells, e_ref, f_ref, w_f, norm_mode=1, pbc=True):
+        """Energy+force loss, its weight gradient, and the model's E and F."""
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        S = len(atom_off) - 1
+        N = int(atom_off[-1])
+        cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(S, 9)
+        e_ref = np.ascontiguousarray(e_ref, dtype=np.float64)
+        f_ref = np.ascontiguousarray(f_ref, dtype=np.float64).reshape(-1, 3)
+        b = _Batch(S, atom_off.ctypes.data, pos.ctypes.data, types.ctypes.data, cells.ctypes.data, 1 if pbc else 0)
+        loss = np.zeros(1)
+        g = np.zeros(self.nparams())
+        eo = np.zeros(S)
+        fo = np.zeros((N, 3))
+        self._check(lib().nnp_train_grad(self._h, C.byref(b), _ptr(e_ref), _ptr(f_ref), float(w_f), norm_mode,
+                                         _ptr(loss), _ptr(g), _ptr(eo), _ptr(fo), 0))
+        return float(loss[0]), g, eo, fo

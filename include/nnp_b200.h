@@ -1,0 +1,157 @@
+/*
+ * nnp_b200.h -- C ABI of the B200 NNP energy/force library (libnnp_b200.so).
+ *
+ * This is the drop-in boundary for the Behler-Parrinello NNP hot path of the
+ * reference (markdellostritto/ace): neighbour list -> radial/angular symmetry
+ * functions -> per-element atomic networks -> analytic forces, plus the
+ * weight gradient of the energy(+force) training loss.  Each entry point names
+ * the reference interface it replaces (paths inside the reference's src/).
+ *
+ * Conventions
+ *  - Every function returns an int status: NNP_OK (0) or a negative NNP_ERR_*
+ *    code; nothing throws across the ABI.  nnp_last_error() gives the message.
+ *  - A handle owns its device memory and one CUDA stream; it is not shared
+ *    between host threads.  Device buffers grow monotonically.
+ *  - Positions, cells and outputs are FP64 on the host side; the device path
+ *    computes in FP32 (or BF16 network layers) with FP64 accumulation of forces
+ *    and per-structure energies.
+ *  - Structures are passed as a CSR batch (nnp_batch).  Atom types are NNP
+ *    type indices (nnp_type_index), i.e. the reference's map_ (nnp.hpp:68).
+ */
+#ifndef NNP_B200_H
+#define NNP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define NNP_OK 0
+#define NNP_ERR_ARG (-1)          /* bad argument (null pointer, bad size, bad flag)      */
+#define NNP_ERR_IO (-2)           /* file could not be opened                             */
+#define NNP_ERR_PARSE (-3)        /* potential / basis file malformed                     */
+#define NNP_ERR_CUDA (-4)         /* CUDA runtime error                                   */
+#define NNP_ERR_CAPACITY (-5)     /* an internal capacity was exceeded and could not grow */
+#define NNP_ERR_UNSUPPORTED (-6)  /* a feature the device path does not implement         */
+#define NNP_ERR_TYPE (-7)         /* atom type index out of range                         */
+#define NNP_ERR_NOT_FINITE (-8)   /* a non-finite energy or force was produced            */
+
+/* ---- precision of the atomic-network layers ---- */
+#define NNP_PREC_FP32 0           /* FP32 CUDA-core network layers (plain path)                   */
+#define NNP_PREC_BF16 1           /* BF16 tensor-core layers, FP32 accumulation (tcgen05, sm_100a) */
+#define NNP_PREC_BF16X3 2         /* split-BF16 (hi/lo, 3 products) tensor-core layers            */
+
+/* ---- nnp_compute flags ---- */
+#define NNP_ENERGY 1u             /* write per-structure energies                                */
+#define NNP_FORCES 2u             /* write forces                                                */
+#define NNP_VACUUM 4u             /* add per-type vacuum energies (NNP::compute_energy semantics) */
+#define NNP_DEVICE_PTRS 8u        /* every pointer in the batch and outputs is device memory     */
+#define NNP_SYMM 16u              /* write the symmetry-function rows (symm_out)                 */
+
+/* CSR batch of periodic (or free) structures.
+ *  atom_off[n_struct+1]  atoms of structure s are [atom_off[s], atom_off[s+1])
+ *  pos[3*N]              Cartesian positions, x y z per atom
+ *  type[N]               NNP type index of each atom
+ *  cell[9*n_struct]      lattice vectors of structure s: cell[9s+3n+d] is
+ *                        component d of vector n, i.e. Cell::R (struc/cell.hpp:23,
+ *                        lattice vectors as columns) stored column-major
+ *  pbc                   nonzero: periodic in all three directions;
+ *                        zero: free boundaries (cell ignored)                   */
+typedef struct {
+    int32_t n_struct;
+    const int64_t *atom_off;
+    const double *pos;
+    const int32_t *type;
+    const double *cell;
+    int32_t pbc;
+} nnp_batch;
+
+typedef struct nnp_handle nnp_handle;
+
+/* Reads a potential file; replaces NNP::read(const char*, NNP&) (src/nnp/nnp.cpp:181-190,
+ * format nnp.cpp:243-307) and uploads it to the current CUDA device. */
+int nnp_create_from_file(const char *potential_path, nnp_handle **out);
+
+/* Builds a potential from its pieces the way nnptefr does (nnptefr.cpp:2023-2031):
+ * type lines as in the potential file (nnh.cpp:65-93), the global cutoff, one
+ * per-element basis file each (NNP::read_basis, nnp.cpp:96-156, written by
+ * make_basis), and one network description per element given as a text block in
+ * the ANN file format (ml/nn.cpp:1536-1613). */
+int nnp_create_from_basis(int32_t ntypes, const char *const *type_lines, double rc,
+                          const char *const *basis_paths, const char *const *network_texts,
+                          nnp_handle **out);
+
+/* Releases the handle and all its device memory. */
+int nnp_destroy(nnp_handle *h);
+
+/* Writes the potential; replaces NNP::write(const char*, const NNP&) (nnp.cpp:165-236). */
+int nnp_write(const nnp_handle *h, const char *path);
+
+/* Network-layer precision (NNP_PREC_*). */
+int nnp_set_precision(nnp_handle *h, int32_t precision);
+
+/* Launch on this CUDA stream (cudaStream_t) instead of the handle's own one. */
+int nnp_set_stream(nnp_handle *h, void *cuda_stream);
+
+/* ---- inspection: NNP::ntypes / index / rc / NNH::nInput (nnp.hpp:78-87, nnh.hpp:140-142) ---- */
+int nnp_ntypes(const nnp_handle *h, int32_t *ntypes);
+int nnp_type_index(const nnp_handle *h, const char *name, int32_t *index);
+int nnp_rc(const nnp_handle *h, double *rc);
+int nnp_n_input(const nnp_handle *h, int32_t type, int32_t *n_input);
+
+/* Energies, forces and (optionally) symmetry functions of a batch.
+ * Replaces NNP::compute(Structure&) (nnp.cpp:489-494) = NeighborList::build
+ * (struc/neighbor.cpp:46-87) + NNP::compute_symm (nnp.cpp:350-392) +
+ * NNP::compute_force (nnp.cpp:412-476), and NNP::compute_energy (nnp.cpp:329-338)
+ * when NNP_VACUUM is set.
+ *  energy[n_struct]   sum of atomic energies (plus vacuum energies with NNP_VACUUM)
+ *  forces[3*N]        -dE/dr per atom
+ *  symm_out[N*gstride] symmetry functions, row per atom, gstride = max n_input
+ *                      (only with NNP_SYMM)
+ * With NNP_DEVICE_PTRS all pointers (batch arrays and outputs) are device
+ * pointers and nothing is copied; otherwise they are host pointers. */
+int nnp_compute(nnp_handle *h, const nnp_batch *batch, double *energy, double *forces,
+                double *symm_out, uint32_t flags);
+
+/* Energy of every structure from precomputed symmetry functions; replaces
+ * NNP::compute_energy (nnp.cpp:329-338) with NNH::energy (nnh.cpp:207-210):
+ * sum over atoms of network(G) + vacuum energy.  symm is N*gstride (host). */
+int nnp_compute_energy_symm(nnp_handle *h, int32_t n_struct, const int64_t *atom_off,
+                            const int32_t *type, const double *symm, int32_t gstride,
+                            double *energy);
+
+/* Number of network parameters of one type / of all types (ANN::size, ml/nn.cpp:1000-1006). */
+int nnp_nparams(const nnp_handle *h, int32_t type, int32_t *n);
+
+/* All networks' parameters, types in index order, each in the reference packing
+ * (biases by layer, then column-major weights): operator>> / operator<<
+ * (ml/nn.cpp:881-915) as used by nnptefr (nnptefr.cpp:1171-1181). */
+int nnp_get_params(const nnp_handle *h, double *params);
+int nnp_set_params(nnp_handle *h, const double *params);
+
+/* Energy(+force) loss and its gradient with respect to all network parameters.
+ * The energy term is NNPTEFR::error_cost_o1's MSE term (nnptefr.cpp:1292-1347,
+ * batch average nnptefr.cpp:996-1000); the force term has no reference
+ * counterpart (nnptefr trains on energies only):
+ *   L = (1/B) sum_s [ 0.5*(norm_s*(E_s - e_ref_s))^2
+ *                     + w_f * 0.5/(3 N_s) * sum_i |F_i - f_ref_i|^2 ]
+ * E_s excludes vacuum energies (nnptefr subtracts them from the labels,
+ * nnptefr.cpp:2958).  norm_mode: 0 IDENTITY, 1 LINEAR (1/N_s), 2 SQRT, 3 CBRT,
+ * 4 LOG (nnptefr.cpp:614-620).  grad has nnp_nparams total entries in the
+ * nnp_get_params order.  e_out / f_out (optional) receive the model's E, F. */
+int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
+                   const double *f_ref, double w_f, int32_t norm_mode, double *loss,
+                   double *grad, double *e_out, double *f_out, uint32_t flags);
+
+/* Message of the last error on this handle (or of the last failed create when h is NULL). */
+const char *nnp_last_error(const nnp_handle *h);
+
+/* Library version string. */
+const char *nnp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,186 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle on
+the same potential file and the same structures.
+
+Tolerances of the FP32 path (stated per quantity, all against the FP64
+oracle): symmetry functions 2e-5 relative to the largest |G| of the atom,
+energy per atom 2e-6 eV, forces 2e-5 eV/A (absolute, largest component)."""
+import numpy as np
+import pytest
+
+from ace_b200 import NNP, NNPError, potential, synth
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+G_RTOL = 2e-5
+E_ATOL = 2e-6     # eV per atom
+F_ATOL = 2e-5     # eV/A
+
+
+def make_pot(tmp_path, k, batch=None, seed=1234):
+    pot = synth.potential_config(k, seed=seed)
+    path = str(tmp_path / ("pot%d.nnp" % k))
+    potential.write(path, pot)
+    b = batch if batch is not None else small_batch(k)
+    op = orc.OraclePot.from_file(path)
+    G = np.concatenate([orc.compute_symm(op, *b.structure(s)) for s in range(b.n_struct)])
+    synth.condition(pot, G, b.type)
+    potential.write(path, pot)
+    return path
+
+
+def small_batch(k, n=6, seed=3):
+    ntypes = {1: 1, 2: 3, 3: 2, 4: 2, 5: 4}[k]
+    rng = np.random.default_rng(seed + k)
+    counts = rng.integers(8, 80, size=n)
+    return synth.batch_random(seed + k, counts, ntypes)
+
+
+def compare(path, b, vacuum=False):
+    op = orc.OraclePot.from_file(path)
+    nn = NNP.read(path)
+    E, F, G = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell, True, symm=True, vacuum=vacuum)
+    Eo, Fo, Go = orc.compute_batch(op, b, want_symm=True)
+    if vacuum:
+        vac = np.array([float(t.split("energy")[1].split()[0]) for t in
+                        [l for l in open(path).read().splitlines() if l.startswith("name ")]])
+        Eo = Eo + np.array([vac[b.type[b.atom_off[s]:b.atom_off[s + 1]]].sum() for s in range(b.n_struct)])
+    nat = np.diff(b.atom_off)
+    gs = Go.shape[1]
+    scale = np.maximum(np.abs(Go).max(axis=1, keepdims=True), 1e-30)
+    g_err = (np.abs(G[:, :gs] - Go) / scale).max()
+    e_err = (np.abs(E - Eo) / nat).max()
+    f_err = np.abs(F - Fo).max()
+    return g_err, e_err, f_err, (E, F, G, Eo, Fo, Go)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_parity_configs(tmp_path, k):
+    b = synth.config1() if k == 1 else small_batch(k)
+    path = make_pot(tmp_path, k, b)
+    g_err, e_err, f_err, _ = compare(path, b)
+    print("config %d: G rel %.2e  E/atom %.2e eV  F %.2e eV/A" % (k, g_err, e_err, f_err))
+    assert g_err < G_RTOL
+    assert e_err < E_ATOL
+    assert f_err < F_ATOL
+
+
+def test_parity_vacuum_energy(tmp_path):
+    b = small_batch(5)
+    path = make_pot(tmp_path, 5, b)
+    g_err, e_err, f_err, _ = compare(path, b, vacuum=True)
+    assert e_err < E_ATOL
+
+
+def test_small_cells_and_self_images(tmp_path):
+    """Cells narrower than rc (self images, several images per atom), triclinic."""
+    b = synth.batch_random(31, [1, 2, 3, 5, 8], 2, density=0.05)
+    path = make_pot(tmp_path, 3, b)
+    g_err, e_err, f_err, _ = compare(path, b)
+    assert g_err < G_RTOL and e_err < E_ATOL and f_err < F_ATOL
+
+
+def test_free_boundaries(tmp_path):
+    b = small_batch(2, n=3)
+    b = synth.Batch(b.atom_off, b.pos, b.type, b.cell, pbc=False)
+    path = make_pot(tmp_path, 2, small_batch(2))
+    op = orc.OraclePot.from_file(path)
+    nn = NNP.read(path)
+    E, F = nn.compute_batch(b.atom_off, b.pos, b.type, None, pbc=False)
+    for s in range(b.n_struct):
+        p, t, c = b.structure(s)
+        eo, fo, _ = orc.compute(op, p, t, np.zeros((3, 3)), pbc=False)
+        assert abs(E[s] - eo) / len(p) < E_ATOL
+        assert np.abs(F[b.atom_off[s]:b.atom_off[s + 1]] - fo).max() < F_ATOL
+
+
+def test_empty_and_ragged(tmp_path):
+    """Empty structures inside a batch and single-atom structures."""
+    b = small_batch(2, n=4)
+    parts = [b.subset([0]), synth.batch_random(40, [1], 3), b.subset([1, 2])]
+    pos = np.concatenate([x.pos for x in parts])
+    typ = np.concatenate([x.type for x in parts])
+    cells = np.concatenate([parts[0].cell, parts[1].cell, parts[1].cell, parts[2].cell])
+    counts = [parts[0].n_atoms, parts[1].n_atoms, 0] + list(np.diff(parts[2].atom_off))
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    bb = synth.Batch(off, pos, typ, cells)
+    path = make_pot(tmp_path, 2, b)
+    nn = NNP.read(path)
+    op = orc.OraclePot.from_file(path)
+    E, F = nn.compute_batch(bb.atom_off, bb.pos, bb.type, bb.cell)
+    Eo, Fo = orc.compute_batch(op, bb)
+    assert E[2] == 0.0
+    np.testing.assert_allclose(E, Eo, atol=E_ATOL * 80)
+    assert np.abs(F - Fo).max() < F_ATOL
+
+
+def test_errors(tmp_path):
+    path = make_pot(tmp_path, 2)
+    nn = NNP.read(path)
+    b = small_batch(2, n=2)
+    bad = b.type.copy()
+    bad[3] = 7
+    with pytest.raises(NNPError) as ei:
+        nn.compute_batch(b.atom_off, b.pos, bad, b.cell)
+    assert ei.value.code == -7
+    with pytest.raises(NNPError) as ei:
+        NNP.read(str(tmp_path / "missing.nnp"))
+    assert ei.value.code == -2
+    with pytest.raises(NNPError) as ei:
+        nn.compute_batch(np.array([0, 5, 3]), b.pos, b.type, b.cell[:2])
+    assert ei.value.code == -1
+
+
+def test_write_roundtrip(tmp_path):
+    path = make_pot(tmp_path, 5)
+    nn = NNP.read(path)
+    out = str(tmp_path / "w.nnp")
+    nn.write(out)
+    assert open(out).read() == open(path).read()
+    assert nn.ntypes == 4 and nn.index("C") == 2 and nn.rc == 6.0
+
+
+def test_params_roundtrip(tmp_path):
+    path = make_pot(tmp_path, 3)
+    nn = NNP.read(path)
+    p = nn.get_params()
+    ref = potential.read(path).get_params()
+    np.testing.assert_array_equal(p, ref)
+    b = small_batch(3, n=2)
+    E0, _ = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    nn.set_params(p * 1.01)
+    E1, _ = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    assert np.abs(E1 - E0).max() > 1e-6
+    nn.set_params(p)
+    E2, _ = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    np.testing.assert_array_equal(E0, E2)
+
+
+def test_compute_energy_from_symm(tmp_path):
+    path = make_pot(tmp_path, 2)
+    nn = NNP.read(path)
+    op = orc.OraclePot.from_file(path)
+    b = small_batch(2, n=1)
+    p, t, c = b.structure(0)
+    G = orc.compute_symm(op, p, t, c)
+    e = nn.compute_energy(t, G)
+    eo = orc.compute_energy(op, t, G)
+    assert abs(e - eo) / len(t) < E_ATOL
+
+
+def test_full_size_properties(tmp_path):
+    """Config-2-sized batch: momentum conservation (sum of forces per structure
+    vanishes) and invariance of energies under a rigid shift + lattice wrap."""
+    b = synth.config2(n_struct=512)
+    path = make_pot(tmp_path, 2, b.subset(range(8)))
+    nn = NNP.read(path)
+    E, F = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    for s in range(0, b.n_struct, 37):
+        fs = F[b.atom_off[s]:b.atom_off[s + 1]]
+        assert np.abs(fs.sum(axis=0)).max() < 1e-4 * max(1.0, np.abs(fs).max())
+    shift = np.concatenate([np.repeat(b.cell[s][0][None] * 1.0 + 0.37, b.atom_off[s + 1] - b.atom_off[s], 0)
+                            for s in range(b.n_struct)])
+    E2, F2 = nn.compute_batch(b.atom_off, b.pos + shift, b.type, b.cell)
+    nat = np.diff(b.atom_off)
+    assert (np.abs(E2 - E) / nat).max() < 1e-5
+    assert np.abs(F2 - F).max() < 1e-4
