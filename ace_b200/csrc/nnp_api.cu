@@ -65,6 +65,7 @@ void Engine::free_all()
     atom_off.release(); pos.release(); cell.release(); xw.release();
     type.release(); atom_struct.release(); atom_cell.release(); grid.release();
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
+    cell_pos.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release();
     if (d_pot) cudaFree(d_pot);
@@ -77,6 +78,9 @@ void Engine::free_all()
     if (own_stream && stream) cudaStreamDestroy(stream);
     stream = nullptr;
     own_stream = false;
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : ev) e = nullptr;
 }
 
 // Build the device potential.  Angular functions of one BasisA that form a
@@ -652,6 +656,58 @@ int nnp_compute_energy_symm(nnp_handle *h, int32_t n_struct, const int64_t *atom
     chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * n_struct, cudaMemcpyDeviceToHost, E.stream));
     chk(cudaStreamSynchronize(E.stream));
     if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("compute_energy failed: ") + cudaGetErrorString(ce));
+    return NNP_OK;
+}
+
+int nnp_set_timing(nnp_handle *h, int32_t enable)
+{
+    if (!h) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (enable && !E.ev[0])
+        for (auto &e : E.ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return fail(h, NNP_ERR_CUDA, "cudaEventCreate failed");
+    E.timing = enable != 0;
+    return NNP_OK;
+}
+
+int nnp_stage_times(const nnp_handle *h, float *ms, int32_t n)
+{
+    if (!h || !ms || n < 0) return NNP_ERR_ARG;
+    const nnp::Engine &E = h->E;
+    for (int k = 0; k < n; ++k) ms[k] = 0.f;
+    if (!E.timing) return NNP_OK;
+    for (int k = 0; k < n && k < 5; ++k) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, E.ev[k], E.ev[k + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            t = 0.f;
+        }
+        ms[k] = t;
+    }
+    return NNP_OK;
+}
+
+int nnp_neighbor_counts(nnp_handle *h, int32_t *counts)
+{
+    if (!h || !counts) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    const size_t n = (size_t)E.n_atoms * E.dpot.ntypes;
+    if (n == 0) return NNP_OK;
+    int *d = nullptr;
+    if (cudaMalloc((void **)&d, n * sizeof(int)) != cudaSuccess) return fail(h, NNP_ERR_CUDA, "cudaMalloc failed");
+    std::string msg = nnp::run_neighbor_counts(E, d);
+    cudaError_t ce = cudaMemcpyAsync(counts, d, n * sizeof(int), cudaMemcpyDeviceToHost, E.stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E.stream);
+    cudaFree(d);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, cudaGetErrorString(ce));
+    return NNP_OK;
+}
+
+int nnp_launch_count(const nnp_handle *h, int64_t *n)
+{
+    if (!h || !n) return NNP_ERR_ARG;
+    *n = h->E.launches;
     return NNP_OK;
 }
 

@@ -81,6 +81,7 @@ struct Engine {
     DBuf<int> type, atom_struct, atom_cell;
     DBuf<StructGrid> grid;
     DBuf<int> cell_cnt, cell_start, cell_fill, cell_atoms, scan_tmp;
+    DBuf<double4> cell_pos;       // cell-ordered wrapped positions, type in .w
     DBuf<float4> nbr;
     DBuf<int> nbr_cnt;
     DBuf<float> G, dEdG, e_atom;
@@ -92,6 +93,15 @@ struct Engine {
     size_t h_stage_bytes = 0;
 
     std::string last_error;
+
+    // stage timers and launch counter
+    bool timing = false;
+    cudaEvent_t ev[6] = {};
+    int64_t launches = 0;
+    void mark(int k)
+    {
+        if (timing && ev[k]) cudaEventRecord(ev[k], stream);
+    }
 
     // build the device potential from `host`
     std::string upload();
@@ -107,5 +117,6 @@ std::string run_force(Engine &E);
 std::string run_energy(Engine &E, bool vacuum);
 std::string run_symm_to_double(Engine &E, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
+std::string run_neighbor_counts(Engine &E, int *d_counts);
 
 }  // namespace nnp

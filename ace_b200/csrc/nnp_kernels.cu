@@ -28,6 +28,7 @@ namespace nnp {
 #define FULL 0xffffffffu
 #define WARPS 8
 #define SYMM_CHUNK 8   // angular functions accumulated in registers per pass
+#define SYMM_CHUNK 8   // angular functions accumulated in registers per pass
 
 __device__ __forceinline__ float warp_sum(float v)
 {
@@ -241,14 +242,25 @@ __global__ void k_sort_cells(const StructGrid *__restrict__ grid, const int *__r
     }
 }
 
+// cell-ordered copy of the wrapped positions with the atom's type in .w, so the
+// neighbour search reads each cell's members contiguously
+__global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const double *__restrict__ xw,
+                           const int *__restrict__ type, double4 *__restrict__ cell_pos)
+{
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const int a = cell_atoms[s];
+    cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2], (double)type[a]);
+}
+
 // one warp per atom.  Candidates are the members of the (2m+1)^3 cells around
 // the atom's cell, each with its lattice image shift; the FP64 displacement
 // x_i - (x_j + R q) decides membership (r^2 < rc^2; a self image needs
 // r^2 > 1e-12 as in neighbor.cpp:78).  The accepted list keeps candidate order
 // and is written grouped by neighbour type: float4(dx,dy,dz, j | type<<28).
-__global__ void __launch_bounds__(WARPS * 32) k_neigh(int64_t N, const int *__restrict__ atom_struct,
+__global__ void __launch_bounds__(WARPS * 32, 3) k_neigh(int64_t N, const int *__restrict__ atom_struct,
                                                      const int *__restrict__ atom_cell, const StructGrid *__restrict__ grid,
-                                                     const double *__restrict__ xw, const int *__restrict__ type,
+                                                     const double *__restrict__ xw, const double4 *__restrict__ cell_pos,
                                                      const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
                                                      const int *__restrict__ cell_atoms, double rc2, int cap, int ntypes,
                                                      float4 *__restrict__ nbr, int *__restrict__ nbr_cnt, DevErr *err)
@@ -303,16 +315,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_neigh(int64_t N, const int *__re
                 const double Q0 = __shfl_sync(FULL, q0, lo), Q1 = __shfl_sync(FULL, q1, lo), Q2 = __shfl_sync(FULL, q2, lo);
                 bool acc = false;
                 float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-                int j = 0;
+                int j = 0, tj = 0;
                 if (k < total) {
-                    j = cell_atoms[st + k - ex];
-                    const double dx = xi0 - (xw[3 * (int64_t)j] + (g.R[0] * Q0 + g.R[3] * Q1 + g.R[6] * Q2));
-                    const double dy = xi1 - (xw[3 * (int64_t)j + 1] + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
-                    const double dz = xi2 - (xw[3 * (int64_t)j + 2] + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
+                    const int slot = st + k - ex;
+                    j = cell_atoms[slot];
+                    const double4 xj = cell_pos[slot];
+                    const double dx = xi0 - (xj.x + (g.R[0] * Q0 + g.R[3] * Q1 + g.R[6] * Q2));
+                    const double dy = xi1 - (xj.y + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
+                    const double dz = xi2 - (xj.z + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
                     const double r2 = dx * dx + dy * dy + dz * dz;
                     if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12)) {
                         acc = true;
                         e = make_float4((float)dx, (float)dy, (float)dz, 0.f);
+                        tj = (int)xj.w;
                     }
                 }
                 const unsigned bal = __ballot_sync(FULL, acc);
@@ -320,7 +335,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_neigh(int64_t N, const int *__re
                 if (acc && p < NNP_MAX_NBR) {
                     s_lst[warp][p] = e;
                     s_j[warp][p] = j;
-                    s_t[warp][p] = (unsigned char)type[j];
+                    s_t[warp][p] = (unsigned char)tj;
                 }
                 count += __popc(bal);
             }
@@ -350,43 +365,48 @@ __global__ void __launch_bounds__(WARPS * 32) k_neigh(int64_t N, const int *__re
 
 // ------------------------------------------------------------------ per-atom staging
 
-// Per-warp shared-memory view of one atom's neighbours (structure of arrays).
+// Per-warp shared-memory view of one atom's neighbours.
 struct NbrView {
-    float *ux, *uy, *uz, *r;
-    int *j;
-    unsigned char *t;
-    float *fc, *fd;     // [ncut][C]
-    float *w, *wd;      // [ndamp][C]
-    float *gx, *gy, *gz;
+    float4 *u;          // unit vector to the neighbour and distance (ux, uy, uz, r) [C]
     float4 *par;        // block parameters [NNP_MAX_AFUNC]
-    float *vec;         // G or dE/dG row [gstride]
-    int *seg;           // [NNP_MAX_TYPES+1] segment starts
+    int *j;             // neighbour atom index [C]
+    float *fc, *fd;     // cutoff value / slope [ncut][C]
+    float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr [ndamp][C]
+    float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
+    float *vec;         // dE/dG row [gstride]
+    float *pc;          // pair coefficients [4][PCH]
+    int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
+    unsigned char *t;   // neighbour type [C]
 };
 
-__host__ __device__ inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride)
+#define PCH 256         // pairs per force chunk
+
+__host__ __device__ inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
 {
-    // ux uy uz r j(t packed as bytes) fc fd w wd gx gy gz, params, vec, seg
-    return C * (4 + 1 + 2 * ncut + 2 * ndamp + 3) + (C + 3) / 4 + 4 * NNP_MAX_AFUNC + gstride + NNP_MAX_TYPES + 1;
+    return 4 * C + 4 * NNP_MAX_AFUNC + C + 2 * ncut * C + 2 * ndamp * C + (force ? 3 * C + gstride + 4 * PCH : 0) +
+           NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
-__device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride)
+__device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
 {
     NbrView v;
     float *p = base;
-    v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;   // 16-byte aligned first
-    v.ux = p; p += C;
-    v.uy = p; p += C;
-    v.uz = p; p += C;
-    v.r = p; p += C;
+    v.u = reinterpret_cast<float4 *>(p); p += 4 * C;                 // 16-byte aligned first
+    v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
     v.j = reinterpret_cast<int *>(p); p += C;
     v.fc = p; p += ncut * C;
     v.fd = p; p += ncut * C;
     v.w = p; p += ndamp * C;
     v.wd = p; p += ndamp * C;
-    v.gx = p; p += C;
-    v.gy = p; p += C;
-    v.gz = p; p += C;
-    v.vec = p; p += gstride;
+    if (force) {
+        v.gx = p; p += C;
+        v.gy = p; p += C;
+        v.gz = p; p += C;
+        v.vec = p; p += gstride;
+        v.pc = p; p += 4 * PCH;
+    } else {
+        v.gx = v.gy = v.gz = v.vec = v.pc = nullptr;
+    }
     v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
     v.t = reinterpret_cast<unsigned char *>(p);
     return v;
@@ -403,10 +423,7 @@ __device__ inline int stage_neighbors(const NbrView &v, int64_t i, int cap, cons
         const float4 e = nbr[i * cap + k];
         const float r = sqrtf(e.x * e.x + e.y * e.y + e.z * e.z);
         const float ir = 1.f / r;
-        v.ux[k] = e.x * ir;
-        v.uy[k] = e.y * ir;
-        v.uz[k] = e.z * ir;
-        v.r[k] = r;
+        v.u[k] = make_float4(e.x * ir, e.y * ir, e.z * ir, r);
         const int pk = __float_as_int(e.w);
         v.j[k] = pk & 0x0fffffff;
         v.t[k] = (unsigned char)((unsigned)pk >> 28);
@@ -425,7 +442,7 @@ __device__ inline int stage_neighbors(const NbrView &v, int64_t i, int cap, cons
             v.wd[d * cap + k] = (g - 2.f * a * r * f) * ex;
         }
     }
-    // type segment starts (list is grouped by type)
+    // type segment starts (the list is grouped by type)
     for (int t = 0; t <= P.ntypes; ++t) {
         int c = 0;
         for (int kb = 0; kb < n; kb += 32) {
@@ -438,31 +455,25 @@ __device__ inline int stage_neighbors(const NbrView &v, int64_t i, int cap, cons
     return n;
 }
 
-// first (a,b) of a lane in a block's pair list and the advance by 32:
-// rectangle rows x cols (J != K) or lower triangle a > b of one segment (J == K)
-struct PairIter {
-    int a, b;
-};
-
-__device__ __forceinline__ void pair_first(bool tri, int cols, int lane, PairIter &p)
+// Pairs of one (J,K) block, segment-local: rectangle a in [0,na) x b in [0,nb)
+// (J != K, index p = a*nb + b) or lower triangle b < a < na (J == K,
+// p = a(a-1)/2 + b).
+__device__ __forceinline__ int tri_row(int p)
 {
-    if (tri) {
-        p.a = 1;
-        p.b = lane;
-        while (p.b >= p.a) { p.b -= p.a; ++p.a; }
-    } else {
-        p.a = lane / cols;
-        p.b = lane - p.a * cols;
-    }
+    int r = (int)((1.f + sqrtf(8.f * (float)p + 1.f)) * 0.5f);
+    if (r * (r - 1) / 2 > p) --r;
+    else if ((r + 1) * r / 2 <= p) ++r;
+    return r;
 }
 
-__device__ __forceinline__ void pair_next(bool tri, int cols, PairIter &p)
+__device__ __forceinline__ void pair_at(bool tri, int nb, int p, int &a, int &b)
 {
-    p.b += 32;
     if (tri) {
-        while (p.b >= p.a) { p.b -= p.a; ++p.a; }
+        a = tri_row(p);
+        b = p - a * (a - 1) / 2;
     } else {
-        while (p.b >= cols) { p.b -= cols; ++p.a; }
+        a = p / nb;
+        b = p - a * nb;
     }
 }
 
@@ -474,18 +485,59 @@ __device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
     J = tt - K * (K + 1) / 2;
 }
 
+// x^n, 0 <= n < 64, by binary powering with branches on the (warp-uniform) bits of n
+__device__ __forceinline__ float upow(float x, int n)
+{
+    float r = (n & 1) ? x : 1.f;
+    if (n >> 1) {
+        x *= x;
+        if (n & 2) r *= x;
+        if (n >> 2) {
+            x *= x;
+            if (n & 4) r *= x;
+            if (n >> 3) {
+                x *= x;
+                if (n & 8) r *= x;
+                if (n >> 4) {
+                    x *= x;
+                    if (n & 16) r *= x;
+                    if (n >> 5) { x *= x; r *= x; }
+                }
+            }
+        }
+    }
+    return r;
+}
+
+// (0.5 + lf cos)^zeta and (.)^(zeta-1), reference form |0.5 + lambda/2 cos|^zeta
+__device__ __forceinline__ void ang_pow(float cs, float lf, float zeta, int iz, float &pz, float &pm1)
+{
+    const float x = fabsf(fmaf(lf, cs, 0.5f));
+    if (iz > 0) {
+        pm1 = upow(x, iz - 1);
+        pz = pm1 * x;
+    } else if (iz == 0) {
+        pm1 = 0.f;
+        pz = 1.f;
+    } else {
+        pm1 = (x > 0.f) ? exp2f((zeta - 1.f) * log2f(x)) : 0.f;
+        pz = pm1 * x;
+    }
+}
+
 // ------------------------------------------------------------------ symmetry functions
 
 __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot *__restrict__ pot,
-                                                    const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
-                                                    const int *__restrict__ type, const float4 *__restrict__ nbr,
-                                                    const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
-                                                    int gstride, float *__restrict__ G)
+                                                       const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
+                                                       const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                       const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
+                                                       int gstride, float *__restrict__ G)
 {
-    extern __shared__ float smem[];
+    extern __shared__ float4 smem4[];
+    float *smem = reinterpret_cast<float *>(smem4);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride);
-    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride);
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, false);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, false);
     const DevPot &P = *pot;
     for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
         const int II = type[i];
@@ -505,13 +557,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
                 float acc = 0.f;
                 for (int k = s0; k < s1; ++k) {
                     float val, der;
-                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
+                    radial_fd(B.form, v.u[k].w, q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
                     acc += val;
                 }
                 Gi[B.off_g + f] = acc;
             }
         }
-        // ---- angular: one block per neighbour-type pair J <= K
+        // ---- angular: one block per neighbour-type pair J <= K, lanes over pairs
         const int TT = P.ntypes * (P.ntypes + 1) / 2;
         for (int tt = 0; tt < TT; ++tt) {
             const DevBlockA B = T.ba[tt];
@@ -523,22 +575,23 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
             const bool tri = (J == K);
             const int npairs = tri ? na * (na - 1) / 2 : na * nb;
             if (npairs == 0) continue;
+            const int sB = tri ? sa : sb;
             for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
             __syncwarp();
             if (B.form == ANG_GAUSS) {
-                // GAUSS: damping exp(-(ra^2+rb^2)/eta^2) fc(ra) fc(rb) = w(ra) w(rb)
-                // from the staged per-neighbour factors; functions in chunks of
-                // SYMM_CHUNK register accumulators
+                // damping exp(-(ra^2+rb^2)/eta^2) fc(ra) fc(rb) = w(ra) w(rb) from the
+                // staged factors; SYMM_CHUNK functions per pass in registers
                 for (int f0 = 0; f0 < B.n; f0 += SYMM_CHUNK) {
                     const int nf = min(SYMM_CHUNK, B.n - f0);
                     float acc[SYMM_CHUNK];
 #pragma unroll
                     for (int f = 0; f < SYMM_CHUNK; ++f) acc[f] = 0.f;
-                    PairIter it;
-                    pair_first(tri, nb, lane, it);
                     for (int p = lane; p < npairs; p += 32) {
-                        const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
-                        const float cs = v.ux[a] * v.ux[b] + v.uy[a] * v.uy[b] + v.uz[a] * v.uz[b];
+                        int ia, ib;
+                        pair_at(tri, nb, p, ia, ib);
+                        const int a = sa + ia, b = sB + ib;
+                        const float4 ua = v.u[a], ub = v.u[b];
+                        const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
                         int dcur = -1;
                         float damp = 0.f;
 #pragma unroll
@@ -551,11 +604,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
                                     dcur = d;
                                     damp = v.w[d * cap + a] * v.w[d * cap + b];
                                 }
-                                const float x = fabsf(0.5f + q.x * cs);
-                                acc[f] += zpow(x, q.y, iz) * damp;
+                                float pz, pm1;
+                                ang_pow(cs, q.x, q.y, iz, pz, pm1);
+                                acc[f] = fmaf(pz, damp, acc[f]);
                             }
                         }
-                        pair_next(tri, nb, it);
                     }
 #pragma unroll
                     for (int f = 0; f < SYMM_CHUNK; ++f) {
@@ -571,16 +624,16 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
                     const float4 q = v.par[f];
                     const int iz = (__float_as_int(q.w) >> 8) - 1;
                     float acc = 0.f;
-                    PairIter it;
-                    pair_first(tri, nb, lane, it);
                     for (int p = lane; p < npairs; p += 32) {
-                        const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
-                        const float cs = v.ux[a] * v.ux[b] + v.uy[a] * v.uy[b] + v.uz[a] * v.uz[b];
+                        int ia, ib;
+                        pair_at(tri, nb, p, ia, ib);
+                        const int a = sa + ia, b = sB + ib;
+                        const float4 ua = v.u[a], ub = v.u[b];
+                        const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
                         float h, hc, hrj, hrk;
-                        angular_generic(B.form, v.r[a], v.r[b], cs, v.fc[B.cut * cap + a], v.fc[B.cut * cap + b], 0.f,
+                        angular_generic(B.form, ua.w, ub.w, cs, v.fc[B.cut * cap + a], v.fc[B.cut * cap + b], 0.f,
                                         0.f, q.x, q.y, iz, q.z, false, h, hc, hrj, hrk);
                         acc += h;
-                        pair_next(tri, nb, it);
                     }
                     acc = warp_sum(acc);
                     if (lane == 0) Gi[B.off_g + f] = acc;
@@ -694,21 +747,26 @@ __global__ void __launch_bounds__(WARPS * 32) k_nn_fp32(int64_t N, const DevPot 
 // ------------------------------------------------------------------ forces
 
 // One warp per atom.  With e = dE_i/dG_i, every pair and triplet contributes
-// dE_i/dd_j for the neighbour displacements d_j = x_i - x_j - R q; the warp
-// accumulates g_j = dE_i/dd_j per neighbour slot, then F_j += g_j and
-// F_i -= sum_j g_j (FP64 atomics) -- the same Newton-3 scatter as
-// nnp.cpp:443-471.
+// dE_i/dd_j for the neighbour displacements d_j = x_i - x_j - R q.  For a
+// triplet (a,b) with dE/dcos = hc, dE/dr_a = hra, dE/dr_b = hrb:
+//   dE/dd_a = (hra - hc cos/r_a) u_a + (hc/r_a) u_b,  and a <-> b.
+// The warp writes these four coefficients per pair of a block into shared
+// memory, then every lane owns neighbour slots and sums their pairs in a
+// fixed order (no atomics).  Finally F_j += g_j and F_i -= sum_j g_j in FP64
+// -- the Newton-3 scatter of nnp.cpp:443-471.
 __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot *__restrict__ pot,
-                                                     const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
-                                                     const int *__restrict__ type, const float4 *__restrict__ nbr,
-                                                     const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
-                                                     int gstride, const float *__restrict__ dEdG,
-                                                     double *__restrict__ F, DevErr *err)
+                                                        const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
+                                                        const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                        const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
+                                                        int gstride, const float *__restrict__ dEdG,
+                                                        double *__restrict__ F, DevErr *err)
 {
-    extern __shared__ float smem[];
+    extern __shared__ float4 smem4[];
+    float *smem = reinterpret_cast<float *>(smem4);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride);
-    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride);
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
+    float *cA = v.pc, *cB = v.pc + PCH, *cC = v.pc + 2 * PCH, *cD = v.pc + 3 * PCH;
     const DevPot &P = *pot;
     for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
         const int II = type[i];
@@ -717,21 +775,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot
         const float *e = dEdG + i * gstride;
         for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
         __syncwarp();
-        // ---- radial: lanes own their neighbour slot
+        // ---- radial: lanes own their neighbour slot (initialises g)
         for (int k = lane; k < n; k += 32) {
             const DevBlockR B = T.br[v.t[k]];
-            const float r = v.r[k];
+            const float4 u = v.u[k];
             const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
             float amp = 0.f;
             for (int f = 0; f < B.n; ++f) {
                 const float2 q = rpar[B.par + f];
                 float val, der;
-                radial_fd(B.form, r, q.x, q.y, fc, fd, val, der);
-                amp += v.vec[B.off_g + f] * der;
+                radial_fd(B.form, u.w, q.x, q.y, fc, fd, val, der);
+                amp = fmaf(v.vec[B.off_g + f], der, amp);
             }
-            v.gx[k] = amp * v.ux[k];
-            v.gy[k] = amp * v.uy[k];
-            v.gz[k] = amp * v.uz[k];
+            v.gx[k] = amp * u.x;
+            v.gy[k] = amp * u.y;
+            v.gz[k] = amp * u.z;
         }
         __syncwarp();
         // ---- angular
@@ -742,86 +800,119 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot
             int J, K;
             tt_decode(tt, J, K);
             const int sa = v.seg[J], na = v.seg[J + 1] - sa;
-            const int sb = v.seg[K], nb = v.seg[K + 1] - sb;
+            const int sb0 = v.seg[K], nb = v.seg[K + 1] - sb0;
             const bool tri = (J == K);
+            const int sb = tri ? sa : sb0;
             const int npairs = tri ? na * (na - 1) / 2 : na * nb;
             if (npairs == 0) continue;
             for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
             __syncwarp();
             const float *eb = v.vec + B.off_g;
             const bool gauss = (B.form == ANG_GAUSS);
-            PairIter it;
-            pair_first(tri, nb, lane, it);
-            for (int p = lane; p < npairs; p += 32) {
-                const int a = sa + it.a, b = (tri ? sa : sb) + it.b;
-                const float uax = v.ux[a], uay = v.uy[a], uaz = v.uz[a];
-                const float ubx = v.ux[b], uby = v.uy[b], ubz = v.uz[b];
-                const float cs = uax * ubx + uay * uby + uaz * ubz;
-                float hc = 0.f, hra = 0.f, hrb = 0.f;   // dE/dcos, dE/dr_a, dE/dr_b
-                if (gauss) {
-                    int dcur = -1;
-                    float sc = 0.f, sp = 0.f;
-#pragma unroll 2
-                    for (int f = 0; f < B.n; ++f) {
-                        {
+            for (int c0 = 0; c0 < npairs; c0 += PCH) {
+                const int c1 = min(npairs, c0 + PCH);
+                // -- pair pass: coefficients of the two per-slot gradients
+                for (int p = c0 + lane; p < c1; p += 32) {
+                    int ia, ib;
+                    pair_at(tri, nb, p, ia, ib);
+                    const int a = sa + ia, b = sb + ib;
+                    const float4 ua = v.u[a], ub = v.u[b];
+                    const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+                    float hc = 0.f, hra = 0.f, hrb = 0.f;   // dE/dcos, dE/dr_a, dE/dr_b
+                    if (gauss) {
+                        int dcur = -1;
+                        float sc = 0.f, sp = 0.f;
+                        for (int f = 0; f < B.n; ++f) {
                             const float4 q = v.par[f];
                             const int pk = __float_as_int(q.w);
                             const int d = pk & 0xff, iz = (pk >> 8) - 1;
                             if (d != dcur) {
                                 if (dcur >= 0) {
                                     const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
-                                    hc += sc * wa * wb;
-                                    hra += sp * v.wd[dcur * cap + a] * wb;
-                                    hrb += sp * wa * v.wd[dcur * cap + b];
+                                    hc = fmaf(sc, wa * wb, hc);
+                                    hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
+                                    hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
                                 }
                                 dcur = d;
                                 sc = 0.f;
                                 sp = 0.f;
                             }
-                            const float x = fabsf(0.5f + q.x * cs);
-                            const float pm1 = (iz > 0) ? ipow(x, iz - 1) : ((iz == 0) ? 0.f : zpow(x, q.y - 1.f, -1));
-                            const float pz = (iz == 0) ? 1.f : pm1 * x;
+                            float pz, pm1;
+                            ang_pow(cs, q.x, q.y, iz, pz, pm1);
                             const float ef = eb[f];
-                            sc += ef * q.y * q.x * pm1;
-                            sp += ef * pz;
+                            sc = fmaf(ef * q.y * q.x, pm1, sc);
+                            sp = fmaf(ef, pz, sp);
                         }
-                    }
-                    if (dcur >= 0) {
-                        const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
-                        hc += sc * wa * wb;
-                        hra += sp * v.wd[dcur * cap + a] * wb;
-                        hrb += sp * wa * v.wd[dcur * cap + b];
-                    }
-                } else {
-                    const float ra = v.r[a], rb = v.r[b];
-                    const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];
-                    const float ga = v.fd[B.cut * cap + a], gb = v.fd[B.cut * cap + b];
-#pragma unroll 1
-                    for (int f = 0; f < B.n; ++f) {
-                        {
+                        if (dcur >= 0) {
+                            const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                            hc = fmaf(sc, wa * wb, hc);
+                            hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
+                            hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
+                        }
+                    } else {
+                        const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];
+                        const float ga = v.fd[B.cut * cap + a], gb = v.fd[B.cut * cap + b];
+                        for (int f = 0; f < B.n; ++f) {
                             const float4 q = v.par[f];
                             const int iz = (__float_as_int(q.w) >> 8) - 1;
                             float h, dc, dra, drb;
-                            angular_generic(B.form, ra, rb, cs, ca, cb, ga, gb, q.x, q.y, iz, q.z, true, h, dc, dra, drb);
+                            angular_generic(B.form, ua.w, ub.w, cs, ca, cb, ga, gb, q.x, q.y, iz, q.z, true, h, dc, dra,
+                                            drb);
                             const float ef = eb[f];
-                            hc += ef * dc;
-                            hra += ef * dra;
-                            hrb += ef * drb;
+                            hc = fmaf(ef, dc, hc);
+                            hra = fmaf(ef, dra, hra);
+                            hrb = fmaf(ef, drb, hrb);
                         }
                     }
+                    const float ira = 1.f / ua.w, irb = 1.f / ub.w;
+                    cA[p - c0] = hra - hc * cs * ira;   // on u_a in dE/dd_a
+                    cB[p - c0] = hc * ira;              // on u_b in dE/dd_a
+                    cC[p - c0] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
+                    cD[p - c0] = hc * irb;              // on u_a in dE/dd_b
                 }
-                const float ira = 1.f / v.r[a], irb = 1.f / v.r[b];
-                const float ca_ = hra - hc * cs * ira, cb_ = hc * ira;
-                atomicAdd(&v.gx[a], ca_ * uax + cb_ * ubx);
-                atomicAdd(&v.gy[a], ca_ * uay + cb_ * uby);
-                atomicAdd(&v.gz[a], ca_ * uaz + cb_ * ubz);
-                const float cc_ = hrb - hc * cs * irb, cd_ = hc * irb;
-                atomicAdd(&v.gx[b], cc_ * ubx + cd_ * uax);
-                atomicAdd(&v.gy[b], cc_ * uby + cd_ * uay);
-                atomicAdd(&v.gz[b], cc_ * ubz + cd_ * uaz);
-                pair_next(tri, nb, it);
+                __syncwarp();
+                // -- slot pass: each lane sums the pairs of the slots it owns
+                const int nslots = tri ? na : na + nb;
+                for (int sl = lane; sl < nslots; sl += 32) {
+                    const bool is_row = tri || sl < na;       // first member of its pairs
+                    const bool is_col = tri || sl >= na;      // second member
+                    const int ir = tri ? sl : sl;             // row index if is_row
+                    const int ic = tri ? sl : sl - na;        // column index if is_col
+                    const int slot = (tri || sl < na) ? sa + sl : sb + ic;
+                    const float4 us = v.u[slot];
+                    float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+                    if (is_row) {
+                        const int rs = tri ? ir * (ir - 1) / 2 : ir * nb;
+                        const int rl = tri ? ir : nb;
+                        const int p0 = max(rs, c0), p1 = min(rs + rl, c1);
+                        for (int p = p0; p < p1; ++p) {
+                            const float4 ub = v.u[sb + (p - rs)];
+                            sa_ += cA[p - c0];
+                            const float bt = cB[p - c0];
+                            vx = fmaf(bt, ub.x, vx);
+                            vy = fmaf(bt, ub.y, vy);
+                            vz = fmaf(bt, ub.z, vz);
+                        }
+                    }
+                    if (is_col) {
+                        for (int ra = tri ? ic + 1 : 0; ra < na; ++ra) {
+                            const int p = (tri ? ra * (ra - 1) / 2 : ra * nb) + ic;
+                            if (p < c0) continue;
+                            if (p >= c1) break;
+                            const float4 ua = v.u[sa + ra];
+                            sa_ += cC[p - c0];
+                            const float dt = cD[p - c0];
+                            vx = fmaf(dt, ua.x, vx);
+                            vy = fmaf(dt, ua.y, vy);
+                            vz = fmaf(dt, ua.z, vz);
+                        }
+                    }
+                    v.gx[slot] += fmaf(sa_, us.x, vx);
+                    v.gy[slot] += fmaf(sa_, us.y, vy);
+                    v.gz[slot] += fmaf(sa_, us.z, vz);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
         __syncwarp();
         // ---- scatter: F_j += g_j, F_i -= sum g_j
@@ -876,6 +967,28 @@ __global__ void k_energy(const int64_t *__restrict__ off, const float *__restric
     }
 }
 
+__global__ void k_nbr_types(int64_t N, const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap,
+                            int ntypes, int *__restrict__ counts)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int c[NNP_MAX_TYPES] = {0};
+    const int n = nbr_cnt[i];
+    for (int k = 0; k < n; ++k) {
+        const unsigned t = (unsigned)__float_as_int(nbr[i * cap + k].w) >> 28;
+        if (t < NNP_MAX_TYPES) c[t]++;
+    }
+    for (int t = 0; t < ntypes; ++t) counts[i * ntypes + t] = c[t];
+}
+
+std::string run_neighbor_counts(Engine &E, int *d_counts)
+{
+    if (E.n_atoms == 0) return "";
+    k_nbr_types<<<grid_for(E.n_atoms, 256, 1 << 30), 256, 0, E.stream>>>(E.n_atoms, E.nbr.p, E.nbr_cnt.p, E.cap,
+                                                                         E.dpot.ntypes, d_counts);
+    return cuda_msg("neighbour counts");
+}
+
 __global__ void k_f2d(int64_t n, const float *__restrict__ a, double *__restrict__ b)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -911,9 +1024,9 @@ static int ndamp_max(const Engine &E)
     return m;
 }
 
-static size_t view_bytes(const Engine &E)
+static size_t view_bytes(const Engine &E, bool force)
 {
-    const int per = nbr_view_floats(E.cap, ncut_max(E), ndamp_max(E), E.gstride);
+    const int per = nbr_view_floats(E.cap, ncut_max(E), ndamp_max(E), E.gstride, force);
     return (size_t)WARPS * ((per + 3) & ~3) * sizeof(float);
 }
 
@@ -935,6 +1048,7 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.cell_start.reserve(cell_bound));
     r(E.cell_fill.reserve(cell_bound));
     r(E.cell_atoms.reserve(N));
+    r(E.cell_pos.reserve(N));
     r(E.nbr.reserve(N * (size_t)E.cap));
     r(E.nbr_cnt.reserve(N));
     r(E.G.reserve(N * (size_t)E.gstride));
@@ -954,6 +1068,8 @@ std::string run_neighbors(Engine &E, int pbc)
     const int S = E.n_struct;
     if (N == 0 || S == 0) return "";
     cudaStream_t st = E.stream;
+    E.mark(0);
+    E.launches += 10;
     k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
                                                              E.dpot.ntypes, E.err.p);
     k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
@@ -966,10 +1082,12 @@ std::string run_neighbors(Engine &E, int pbc)
     k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
     k_sort_cells<<<S, 128, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p);
+    k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     k_neigh<<<grid_for(N, WARPS, num_sms() * 8), WARPS * 32, 0, st>>>(
-        N, E.atom_struct.p, E.atom_cell.p, E.grid.p, E.xw.p, E.type.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p,
+        N, E.atom_struct.p, E.atom_cell.p, E.grid.p, E.xw.p, E.cell_pos.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p,
         rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
+    E.mark(1);
     return cuda_msg("neighbour list");
 }
 
@@ -977,11 +1095,13 @@ std::string run_symm(Engine &E)
 {
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
-    const size_t sm = view_bytes(E);
+    const size_t sm = view_bytes(E, false);
     cudaFuncSetAttribute(k_symm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_symm<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
         N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
         E.G.p);
+    E.launches += 1;
+    E.mark(2);
     return cuda_msg("symmetry functions");
 }
 
@@ -1003,6 +1123,8 @@ std::string run_nn(Engine &E)
     cudaFuncSetAttribute(k_nn_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_nn_fp32<<<grid_for(N, WARPS * 8, num_sms() * 2), WARPS * 32, sm, E.stream>>>(
         N, E.d_pot, E.wpar.p, E.wfloats, E.type.p, E.G.p, E.gstride, maxn, E.e_atom.p, E.dEdG.p);
+    E.launches += 1;
+    E.mark(3);
     return cuda_msg("networks");
 }
 
@@ -1011,11 +1133,13 @@ std::string run_force(Engine &E)
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
     cudaMemsetAsync(E.force.p, 0, 3 * (size_t)N * sizeof(double), E.stream);
-    const size_t sm = view_bytes(E);
+    const size_t sm = view_bytes(E, true);
     cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_force<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
         N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
         E.dEdG.p, E.force.p, E.err.p);
+    E.launches += 1;
+    E.mark(4);
     return cuda_msg("forces");
 }
 
@@ -1024,6 +1148,8 @@ std::string run_energy(Engine &E, bool vacuum)
     if (E.n_struct == 0) return "";
     k_energy<<<E.n_struct, 256, 0, E.stream>>>(E.atom_off.p, E.e_atom.p, E.type.p, E.d_pot, vacuum ? 1 : 0,
                                                E.vac.p, E.e_struct.p, E.err.p);
+    E.launches += 1;
+    E.mark(5);
     return cuda_msg("energies");
 }
 

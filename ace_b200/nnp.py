@@ -64,6 +64,10 @@ def lib():
             "nnp_get_params": ([p, p], i),
             "nnp_set_params": ([p, p], i),
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
+            "nnp_set_timing": ([p, i], i),
+            "nnp_stage_times": ([p, p, i], i),
+            "nnp_neighbor_counts": ([p, p], i),
+            "nnp_launch_count": ([p, C.POINTER(C.c_int64)], i),
             "nnp_last_error": ([p], C.c_char_p),
             "nnp_version": ([], C.c_char_p),
         }
@@ -162,6 +166,28 @@ class NNP:
     def set_stream(self, stream_ptr: int):
         self._check(lib().nnp_set_stream(self._h, C.c_void_p(stream_ptr)))
 
+    # ---- stage timers (the reference's phase clocks) and counters
+    STAGES = ("neighbors", "symm", "networks", "forces", "energies")
+
+    def set_timing(self, on: bool = True):
+        self._check(lib().nnp_set_timing(self._h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        ms = np.zeros(5, dtype=np.float32)
+        self._check(lib().nnp_stage_times(self._h, _ptr(ms), 5))
+        return dict(zip(self.STAGES, (float(x) for x in ms)))
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        self._check(lib().nnp_launch_count(self._h, C.byref(v)))
+        return v.value
+
+    def neighbor_counts(self, n_atoms: int) -> np.ndarray:
+        """[N, ntypes] neighbour counts by type of the last compute call."""
+        c = np.zeros((max(n_atoms, 1), self.ntypes), dtype=np.int32)
+        self._check(lib().nnp_neighbor_counts(self._h, _ptr(c)))
+        return c[:n_atoms]
+
     def nparams(self, t: int = -1) -> int:
         v = C.c_int32()
         self._check(lib().nnp_nparams(self._h, t, C.byref(v)))
@@ -180,8 +206,9 @@ class NNP:
 
     # ---- batched compute
     def compute_batch(self, atom_off, pos, types, cells, pbc=True, energy=True, forces=True,
-                      symm=False, vacuum=False):
-        """Energies [n_struct], forces [N,3] (and symmetry functions [N,gstride]) of a CSR batch."""
+                      symm=False, vacuum=False, out_e=None, out_f=None):
+        """Energies [n_struct], forces [N,3] (and symmetry functions [N,gstride]) of a CSR batch.
+        out_e / out_f may be caller-owned (e.g. pinned) float64 arrays to write into."""
         atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         types = np.ascontiguousarray(types, dtype=np.int32)
@@ -190,8 +217,10 @@ class NNP:
         N = int(atom_off[-1]) if S else 0
         b = _Batch(S, atom_off.ctypes.data, pos.ctypes.data, types.ctypes.data,
                    cells.ctypes.data if cells is not None else None, 1 if pbc else 0)
-        E = np.zeros(max(S, 1))
-        F = np.zeros((max(N, 1), 3))
+        E = out_e if out_e is not None else np.zeros(max(S, 1))
+        F = out_f if out_f is not None else np.zeros((max(N, 1), 3))
+        if E.dtype != np.float64 or not E.flags.c_contiguous or F.dtype != np.float64 or not F.flags.c_contiguous:
+            raise NNPError(-1, "output arrays must be contiguous float64")
         gs = self.gstride
         G = np.zeros((max(N, 1), gs)) if symm else None
         flags = (ENERGY if energy else 0) | (FORCES if forces else 0) | (SYMM if symm else 0) | (VACUUM if vacuum else 0)

@@ -145,6 +145,23 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);
 
+/* Stage timers, the device-side counterpart of the reference's phase clocks
+ * ("time - symm/energy/force", nnptefr.cpp:2863-2885, 3547-3592).  When enabled,
+ * nnp_compute records CUDA events between its stages; nnp_stage_times then
+ * returns the last call's durations in ms: [0] neighbour list, [1] symmetry
+ * functions, [2] networks, [3] forces, [4] energies. */
+int nnp_set_timing(nnp_handle *h, int32_t enable);
+int nnp_stage_times(const nnp_handle *h, float *ms, int32_t n);
+
+/* Neighbour counts of the last nnp_compute, split by neighbour type:
+ * counts[i*ntypes + t] is the number of type-t neighbours of atom i (host
+ * array of N*ntypes).  The pair and triplet counts per atom follow from these
+ * (NeighborList::size, struc/neighbor.hpp:35). */
+int nnp_neighbor_counts(nnp_handle *h, int32_t *counts);
+
+/* Kernels this handle has launched since it was created. */
+int nnp_launch_count(const nnp_handle *h, int64_t *n);
+
 /* Message of the last error on this handle (or of the last failed create when h is NULL). */
 const char *nnp_last_error(const nnp_handle *h);
 
