@@ -65,9 +65,10 @@ void Engine::free_all()
     atom_off.release(); pos.release(); cell.release(); xw.release();
     type.release(); atom_struct.release(); atom_cell.release(); grid.release();
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
-    cell_pos.release();
+    cell_pos.release(); order.release(); type_fill.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release();
+    jit_release(*this);
     if (d_pot) cudaFree(d_pot);
     d_pot = nullptr;
     if (h_err) cudaFreeHost(h_err);
@@ -86,7 +87,7 @@ void Engine::free_all()
 // Build the device potential.  Angular functions of one BasisA that form a
 // run of equal eta (BasisA::init, basis_angular.cpp:178-205) share the run's
 // first eta for their damping factor, as the reference does.
-std::string Engine::upload()
+std::string Engine::build_tables()
 {
     const HostPot &H = host;
     const int T = H.ntypes();
@@ -195,7 +196,23 @@ std::string Engine::upload()
     for (int II = 0; II < T; ++II) gs = std::max(gs, d.t[II].n_input);
     gstride = (gs + 3) & ~3;
     wfloats = (int64_t)wp.size();
+    rpar_host = rp;
+    apar_host = ap;
+    wpar_host = wp;
+    vac_host = vc;
     dpot = d;
+    return "";
+}
+
+std::string Engine::upload()
+{
+    std::string msg = build_tables();
+    if (!msg.empty()) return msg;
+    const DevPot &d = dpot;
+    std::vector<float2> rp = rpar_host;
+    std::vector<float4> ap = apar_host;
+    const std::vector<float> &wp = wpar_host;
+    const std::vector<double> &vc = vac_host;
     if (rp.empty()) rp.push_back(make_float2(0.f, 0.f));
     if (ap.empty()) ap.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
     cudaError_t e = cudaSuccess;
@@ -245,6 +262,14 @@ int finish_create(nnp_handle *h, nnp_handle **out)
         return fail(nullptr, NNP_ERR_CUDA, msg);
     }
     E.cap = 64;
+    // kernels specialised for this basis; NNP_JIT=0 in the environment keeps
+    // the prebuilt kernels (a failed compilation does too, and is recorded)
+    const char *env = std::getenv("NNP_JIT");
+    E.use_jit = !(env && env[0] == '0');
+    if (E.use_jit) {
+        E.jit_error = nnp::jit_build(E);
+        if (!E.jit_error.empty()) E.use_jit = false;
+    }
     *out = h;
     return NNP_OK;
 }
@@ -409,6 +434,70 @@ int nnp_set_precision(nnp_handle *h, int32_t precision)
     if (precision != NNP_PREC_FP32 && precision != NNP_PREC_BF16 && precision != NNP_PREC_BF16X3)
         return fail(h, NNP_ERR_ARG, "unknown precision");
     h->E.precision = precision;
+    return NNP_OK;
+}
+
+int nnp_set_specialization(nnp_handle *h, int32_t enable)
+{
+    if (!h) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (enable && !E.jit_module) {
+        E.jit_error = nnp::jit_build(E);
+        if (!E.jit_error.empty()) {
+            E.use_jit = false;
+            return fail(h, NNP_ERR_CUDA, E.jit_error);
+        }
+    }
+    E.use_jit = enable != 0;
+    return NNP_OK;
+}
+
+int nnp_specialization(const nnp_handle *h, int32_t *active, const char **source)
+{
+    if (!h || !active) return NNP_ERR_ARG;
+    *active = (h->E.use_jit && h->E.jit_module) ? 1 : 0;
+    if (source) *source = h->E.jit_source.c_str();
+    return NNP_OK;
+}
+
+int nnp_specialization_check(const char *potential_path, char *log, int32_t log_len)
+{
+    auto put = [&](const std::string &s) {
+        if (log && log_len > 0) {
+            std::strncpy(log, s.c_str(), (size_t)log_len - 1);
+            log[log_len - 1] = '\0';
+        }
+    };
+    if (!potential_path) return NNP_ERR_ARG;
+    std::string text;
+    if (!read_file(potential_path, text)) {
+        put("could not open potential file");
+        return NNP_ERR_IO;
+    }
+    nnp::Engine E;
+    std::string msg = nnp::read_potential(text, E.host);
+    if (!msg.empty()) {
+        put(msg);
+        return NNP_ERR_PARSE;
+    }
+    msg = E.build_tables();
+    if (!msg.empty()) {
+        put(msg);
+        return NNP_ERR_UNSUPPORTED;
+    }
+    std::string src;
+    std::vector<char> cubin;
+    nnp::jit_last_log().clear();
+    msg = nnp::jit_compile(E, src, cubin);
+    put(msg.empty() ? nnp::jit_last_log() + "\n" + src : msg);
+    return msg.empty() ? NNP_OK : NNP_ERR_CUDA;
+}
+
+int nnp_set_accumulation(nnp_handle *h, int32_t acc)
+{
+    if (!h) return NNP_ERR_ARG;
+    if (acc != NNP_ACC_FP32 && acc != NNP_ACC_FP64) return fail(h, NNP_ERR_ARG, "unknown accumulation mode");
+    h->E.acc64 = (acc == NNP_ACC_FP64);
     return NNP_OK;
 }
 

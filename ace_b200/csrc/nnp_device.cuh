@@ -1,0 +1,1013 @@
+// nnp_device.cuh -- device-side types and building blocks of the NNP path.
+//
+// Shared by the prebuilt kernels (nnp_kernels.cu, nvcc) and the kernels that
+// nnp_jit.cpp specialises at run time for one potential (NVRTC), so it uses
+// plain CUDA C++ only: no host headers, no standard library.
+//
+// Basis functions, cutoffs and activations are FP32 versions of the cited
+// reference formulas; where a reference formula overflows in FP32 (it is
+// written for FP64) the same function is evaluated in an algebraically equal,
+// overflow-free form, which the comment says.  Transcendentals are CUDA's own
+// expf/tanhf/... .
+#pragma once
+
+#define NNP_MAX_TYPES 8
+#define NNP_MAX_TT (NNP_MAX_TYPES * (NNP_MAX_TYPES + 1) / 2)
+#define NNP_MAX_LAYERS 8
+#define NNP_MAX_RFUNC 32      // radial functions in one (centre, neighbour) block
+#define NNP_MAX_AFUNC 32      // angular functions in one (centre, pair) block
+#define NNP_MAX_DAMP 8        // distinct GAUSS damping factors per centre type
+#define NNP_MAX_CUT 4         // distinct (cutoff form, rc) pairs in a potential
+#define NNP_MAX_NODES 128     // widest network layer handled on the device
+#define NNP_MAX_NBR 256       // neighbours per atom staged in shared memory
+
+#define NNP_WARPS 8           // warps per block of the per-atom kernels
+#define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
+#define NNP_PCH 256           // pairs per chunk of the force kernel's pair pass
+#define NNP_FULL 0xffffffffu
+
+#ifdef __CUDACC__
+#define NNP_HD __host__ __device__
+#else
+#define NNP_HD
+#endif
+
+namespace nnp {
+
+typedef long long i64;
+
+// Row stride of a transposed weight matrix W^T (ni x no) in shared memory:
+// odd, so lanes reading a column (fixed n, consecutive m) hit distinct banks.
+NNP_HD inline int wt_stride(int no) { return (no % 2 == 0) ? no + 1 : no + 2; }
+
+// Cutoff::Name, BasisR::Name, BasisA::Name, NN::Neuron numbering of the reference
+enum CutName { CUT_NONE = 0, CUT_STEP, CUT_COS, CUT_TANH, CUT_POLY3 };
+enum RadName { RAD_NONE = 0, RAD_GAUSSIAN, RAD_SECH, RAD_LOGISTIC, RAD_TANH, RAD_LOGCOSH, RAD_LOGCOSH2 };
+enum AngName { ANG_NONE = 0, ANG_GAUSS, ANG_GAUSS2, ANG_SECH, ANG_STUDENT3, ANG_STUDENT4, ANG_STUDENT5 };
+enum Neuron {
+    NEU_NONE = 0, NEU_LINEAR, NEU_SIGMOID, NEU_TANH, NEU_ISRU, NEU_ARCTAN, NEU_RELU, NEU_ELU, NEU_TANHRE,
+    NEU_SQRE, NEU_SWISH, NEU_GELU, NEU_MISH, NEU_PFLU, NEU_LOGISH, NEU_SOFTPLUS, NEU_SQPLUS, NEU_ATISH,
+    NEU_IERF, NEU_TEST
+};
+
+// ---------------------------------------------------------------- device model
+struct DevCut { int name; float rc, rci, pirci; };
+
+struct DevBlockR {
+    int n;        // functions
+    int off_g;    // offset of the block inside G
+    int form;     // RadName
+    int cut;      // index into DevPot::cut
+    int par;      // first function in rpar (float2: rs, eta)
+};
+
+struct DevBlockA {
+    int n;
+    int off_g;    // absolute offset in G (nInputR + offsetA)
+    int form;     // AngName
+    int cut;
+    int par;      // first function in apar (float4: lambdaf, zeta, ieta2, damp | (izeta+1) << 8)
+    int int_zeta; // all zeta are small non-negative integers
+};
+
+struct DevType {
+    int n_input, n_input_r;
+    DevBlockR br[NNP_MAX_TYPES];
+    DevBlockA ba[NNP_MAX_TT];
+    int ndamp;                      // distinct (cutoff, 1/eta^2) GAUSS damping factors
+    float damp_a[NNP_MAX_DAMP];     // 1/eta^2 of the damping factor
+    int damp_cut[NNP_MAX_DAMP];     // its cutoff index
+    int nlayer;
+    int nodes[NNP_MAX_LAYERS + 1];
+    int neuron;
+    float c;
+    i64 woff;                       // first float of this network in wpar
+};
+
+struct DevPot {
+    int ntypes;
+    int ncut;
+    float rc;
+    double rc_d;
+    DevCut cut[NNP_MAX_CUT];
+    DevType t[NNP_MAX_TYPES];
+};
+
+// device error record: kernels raise flags, the host reads them after a step
+struct DevErr {
+    int need_cap;     // largest neighbour count seen (when above the capacity)
+    int bad_type;     // an atom type was outside [0, ntypes)
+    int bad_cell;     // a periodic cell had no volume
+    int nonfinite;    // a non-finite energy or force
+};
+
+#if defined(__CUDACC__)
+
+#define NNP_PI_F 3.14159265358979f
+#define NNP_RAD2_F 1.41421356237310f
+#define NNP_RADPI_F 1.77245385090552f
+#define NNP_LOG2_F 0.69314718055995f
+
+// ---------------------------------------------------------------- math
+
+// Cutoff::cutf / cutg (src/nnp/cutoff.cpp:62-114).  COS uses sincospif, the
+// reference a degree-15/16 Taylor series of cos/sin about pi/2 whose error
+// (<1e-11) is far below FP32 resolution.
+__device__ __forceinline__ void cutoff_fg(const DevCut &c, float r, float &f, float &g)
+{
+    f = 0.f;
+    g = 0.f;
+    if (!(r < c.rc)) return;
+    switch (c.name) {
+    case CUT_STEP: f = 1.f; break;
+    case CUT_COS: {
+        float s, co;
+        sincospif(r * c.rci, &s, &co);
+        f = 0.5f * (co + 1.f);
+        g = -0.5f * c.pirci * s;
+    } break;
+    case CUT_TANH: {
+        const float t = tanhf(1.f - r * c.rci);
+        f = t * t * t;
+        g = -3.f * t * t * (1.f - t * t) * c.rci;
+    } break;
+    case CUT_POLY3: {
+        const float x = r * c.rci;
+        f = (2.f * x - 3.f) * x * x + 1.f;
+        g = 6.f * x * (x - 1.f) * c.rci;
+    } break;
+    default: break;
+    }
+}
+
+// sech(x) and tanh(x) from e = exp(-|x|) (no overflow for any x)
+__device__ __forceinline__ void sech_tanh(float x, float &s, float &t)
+{
+    const float e = expf(-fabsf(x));
+    const float e2 = e * e;
+    const float den = 1.f / (1.f + e2);
+    s = 2.f * e * den;
+    t = copysignf((1.f - e2) * den, x);
+}
+
+// BasisR::symmf / symmd (src/nnp/basis_radial.cpp:175-257): value G(r) and
+// derivative dG/dr of one radial function with cutoff value fc and slope fcd.
+__device__ __forceinline__ void radial_fd(int form, float r, float rs, float eta, float fc, float fcd,
+                                          float &val, float &der)
+{
+    switch (form) {
+    case RAD_GAUSSIAN: {
+        const float arg = eta * (r - rs);
+        const float e = expf(-arg * arg);
+        val = e * fc;
+        der = e * (-2.f * eta * arg * fc + fcd);
+    } break;
+    case RAD_SECH: {            // 2e/(1+e^2) with e=exp(-x) is sech(x)
+        float s, t;
+        sech_tanh(eta * (r - rs), s, t);
+        val = s * fc;
+        der = s * (-eta * t * fc + fcd);
+    } break;
+    case RAD_LOGISTIC: {        // 4e/(1+e)^2 with e=exp(-2x) is sech(x)^2
+        float s, t;
+        sech_tanh(eta * (r - rs), s, t);
+        val = s * s * fc;
+        der = s * s * (-2.f * eta * t * fc + fcd);
+    } break;
+    case RAD_TANH: {
+        const float t = tanhf(-eta * (r - rs));
+        val = 0.5f * (t + 1.f) * fc;
+        der = 0.5f * (-eta * (1.f - t * t) * fc + (1.f + t) * fcd);
+    } break;
+    case RAD_LOGCOSH: {         // 0.5*log1p(exp(y)), y=-2x, as a stable softplus
+        const float y = -2.f * eta * (r - rs);
+        const float sp = (y > 0.f) ? y + log1pf(expf(-y)) : log1pf(expf(y));
+        const float sg = 1.f / (1.f + expf(-y));          // e/(1+e)
+        val = 0.5f * sp * fc;
+        der = -eta * sg * fc + 0.5f * sp * fcd;
+    } break;
+    case RAD_LOGCOSH2: {        // a*e/(e-1) = a/(1-q), e=exp(k a), q=exp(-k a), k=2*sqrt(2)
+        const float k = 2.f * NNP_RAD2_F;
+        const float a = -eta * (r - rs);
+        float f, fa;            // f(a) and df/da
+        if (fabsf(a) < 1e-3f) {
+            f = 1.f / k + 0.5f * a + k * a * a / 12.f;
+            fa = 0.5f + k * a / 6.f;
+        } else {
+            const float q = expf(-k * a);
+            const float om = -expm1f(-k * a);              // 1-q
+            f = a / om;
+            fa = (om - k * a * q) / (om * om);
+        }
+        val = f * fc;
+        der = fa * (-eta) * fc + f * fcd;
+    } break;
+    default: val = 0.f; der = 0.f;
+    }
+}
+
+// x^n for a small non-negative integer n by binary powering
+__device__ __forceinline__ float ipow(float x, int n)
+{
+    float r = 1.f;
+    while (n) {
+        if (n & 1) r *= x;
+        x *= x;
+        n >>= 1;
+    }
+    return r;
+}
+
+__device__ __forceinline__ float zpow(float x, float zeta, int izeta)
+{
+    if (izeta >= 0) return ipow(x, izeta);
+    return (x > 0.f) ? exp2f(zeta * log2f(x)) : ((zeta == 0.f) ? 1.f : 0.f);
+}
+
+// x^n, 0 <= n < 64, by binary powering with branches on the (warp-uniform) bits of n
+__device__ __forceinline__ float upow(float x, int n)
+{
+    float r = (n & 1) ? x : 1.f;
+    if (n >> 1) {
+        x *= x;
+        if (n & 2) r *= x;
+        if (n >> 2) {
+            x *= x;
+            if (n & 4) r *= x;
+            if (n >> 3) {
+                x *= x;
+                if (n & 8) r *= x;
+                if (n >> 4) {
+                    x *= x;
+                    if (n & 16) r *= x;
+                    if (n >> 5) { x *= x; r *= x; }
+                }
+            }
+        }
+    }
+    return r;
+}
+
+// (0.5 + lf cos)^zeta and (.)^(zeta-1), the reference's |0.5 + lambda/2 cos|^zeta
+__device__ __forceinline__ void ang_pow(float cs, float lf, float zeta, int iz, float &pz, float &pm1)
+{
+    const float x = fabsf(fmaf(lf, cs, 0.5f));
+    if (iz > 0) {
+        pm1 = upow(x, iz - 1);
+        pz = pm1 * x;
+    } else if (iz == 0) {
+        pm1 = 0.f;
+        pz = 1.f;
+    } else {
+        pm1 = (x > 0.f) ? exp2f((zeta - 1.f) * log2f(x)) : 0.f;
+        pz = pm1 * x;
+    }
+}
+
+// Angular functions other than GAUSS (BasisA::symmf / symmd,
+// basis_angular.cpp:212-364) for one function: value h and the partials
+// dh/dcos, dh/drj, dh/drk.  cj,ck are cutoff values, gj,gk their slopes.
+__device__ __forceinline__ void angular_generic(int form, float rj, float rk, float cs, float cj, float ck,
+                                                float gj, float gk, float lf, float zeta, int izeta,
+                                                float ieta2, bool want_der, float &h, float &hc,
+                                                float &hrj, float &hrk)
+{
+    const float r2s = rj * rj + rk * rk;
+    const float cw = fabsf(0.5f + lf * cs);
+    const float pm1 = zpow(cw, zeta - 1.f, izeta > 0 ? izeta - 1 : -1);
+    const float pz = (izeta == 0) ? 1.f : pm1 * cw;
+    float rad, dfac;            // radial factor and d(rad)/dr_j = -2 r_j * dfac * rad
+    switch (form) {
+    case ANG_GAUSS: {
+        rad = expf(-ieta2 * r2s);
+        dfac = ieta2;
+    } break;
+    case ANG_GAUSS2: {
+        const float fd = expf(-0.5f * NNP_PI_F * ieta2 * r2s);
+        const float den = 1.f / (1.f + fd);
+        rad = 2.f * fd * den;
+        dfac = 0.5f * NNP_PI_F * ieta2 * den;
+    } break;
+    case ANG_SECH: {
+        const float fd = expf(-0.5f * NNP_PI_F * ieta2 * r2s);
+        const float fd2 = fd * fd, den = 1.f / (1.f + fd2);
+        rad = 2.f * fd * den;
+        dfac = 0.5f * NNP_PI_F * ieta2 * (1.f - fd2) * den;
+    } break;
+    case ANG_STUDENT3: case ANG_STUDENT4: case ANG_STUDENT5: {
+        const int p = 4 + (form - ANG_STUDENT3);
+        const float den = rsqrtf(1.f + ieta2 * r2s);
+        rad = ipow(den, p);
+        dfac = ieta2 * 0.5f * (float)p * den * den;
+    } break;
+    default: rad = 0.f; dfac = 0.f;
+    }
+    h = pz * rad * cj * ck;
+    if (want_der) {
+        hc = zeta * lf * pm1 * rad * cj * ck;
+        hrj = pz * rad * (-2.f * rj * cj * dfac + gj) * ck;
+        hrk = pz * rad * (-2.f * rk * ck * dfac + gk) * cj;
+    }
+}
+
+// AFFPBP activations (src/ml/nn.cpp:148-848): a = f(z), d = f'(z), and
+// d2 = f''(z) (AFFPBP2) for the activations the training path uses.
+__device__ __forceinline__ void activation(int neuron, float c, float z, float &a, float &d, float &d2)
+{
+    d2 = 0.f;
+    switch (neuron) {
+    case NEU_LINEAR: a = z; d = 1.f; break;
+    case NEU_SIGMOID: {
+        const float e = expf(-c * fabsf(z));
+        const float fr = 1.f / (1.f + e);
+        a = (z >= 0.f) ? fr : e * fr;
+        d = c * e * fr * fr;
+        d2 = (z >= 0.f) ? -c * c * e * (1.f - e) * fr * fr * fr : -c * c * e * (e - 1.f) * fr * fr * fr;
+    } break;
+    case NEU_TANH: {
+        const float t = tanhf(c * z);
+        a = t;
+        d = c * (1.f - t * t);
+        d2 = c * c * (-2.f * t * (1.f - t * t));
+    } break;
+    case NEU_ISRU: {
+        const float zz = c * z, isr = rsqrtf(1.f + zz * zz);
+        a = zz * isr;
+        d = c * isr * isr * isr;
+    } break;
+    case NEU_ARCTAN: {
+        const float zz = c * z * NNP_PI_F / 2.f;
+        a = (2.f / NNP_PI_F) * atanf(zz);
+        d = c / (1.f + zz * zz);
+    } break;
+    case NEU_RELU: a = (z > 0.f) ? z : 0.f; d = (z > 0.f) ? 1.f : 0.f; break;
+    case NEU_ELU:
+        if (z >= 0.f) { a = z; d = 1.f; } else { const float e = expf(c * z); a = e - 1.f; d = c * e; }
+        break;
+    case NEU_TANHRE:
+        if (z >= 0.f) { a = z; d = 1.f; } else { const float e = expf(2.f * c * z); a = (e - 1.f) / (e + 1.f); d = c * (1.f - a * a); }
+        break;
+    case NEU_SQRE:
+        if (z >= 0.f) { a = z; d = 1.f; } else { const float den = rsqrtf(1.f + z * z); a = z * den; d = den * den * den; }
+        break;
+    case NEU_SWISH: {
+        const float zz = c * z;
+        if (zz > 0.f) { const float e = expf(-zz), den = 1.f / (1.f + e); a = z * den; d = (1.f + e * (1.f + zz)) * den * den; }
+        else { const float e = expf(zz), den = 1.f / (1.f + e); a = z * e * den; d = e * (1.f + zz + e) * den * den; }
+    } break;
+    case NEU_GELU: {
+        const float zz = 0.5f * NNP_RADPI_F * c * z, ep1 = 1.f + erff(zz);
+        a = 0.5f * z * ep1;
+        d = 0.5f * (ep1 + c * z * expf(-zz * zz));
+    } break;
+    case NEU_MISH: {
+        const float zz = c * z;
+        if (zz > 0.f) {
+            const float e = expf(-zz), e2 = e * e, den = 1.f / ((1.f + e) * (1.f + e) + e2);
+            a = z * (1.f - 2.f * e2 * den);
+            d = 1.f - 2.f * e2 * den * (1.f - 2.f * zz * (1.f + e) * den);
+        } else {
+            const float e = expf(zz), den = 1.f / (e * (e + 2.f) + 2.f);
+            a = z * e * (e + 2.f) * den;
+            d = 1.f + 2.f * den * (-1.f + 2.f * zz * (1.f - (e + 2.f) * den));
+        }
+    } break;
+    case NEU_PFLU: {
+        const float zz = c * z, z2 = zz * zz, fs = rsqrtf(z2 + 1.f);
+        a = 0.5f * z * (1.f + zz * fs);
+        d = 0.5f * (zz * (z2 + 2.f) * fs * fs * fs + 1.f);
+    } break;
+    case NEU_LOGISH: {
+        const float l2i = 1.f / NNP_LOG2_F, e = expf(-z), lf = logf(1.f + 1.f / (1.f + e));
+        a = l2i * z * lf;
+        d = l2i * (lf + z * e / ((1.f + e) * (2.f + e)));
+    } break;
+    case NEU_SOFTPLUS: {
+        const float ci = 1.f / c;
+        if (z > 0.f) { const float e = expf(-c * z); a = z + ci * (log1pf(e) - NNP_LOG2_F); d = 1.f / (e + 1.f); }
+        else { const float e = expf(c * z); a = ci * (log1pf(e) - NNP_LOG2_F); d = e / (e + 1.f); }
+    } break;
+    case NEU_SQPLUS: {
+        const float ci = 1.f / c, zz = c * z, fs = sqrtf(1.f + zz * zz);
+        a = 0.5f * ci * (zz - 1.f + fs);
+        d = 0.5f * (zz / fs + 1.f);
+    } break;
+    case NEU_ATISH: {
+        const float zz = 0.5f * NNP_PI_F * z;
+        a = z * 0.5f * (1.f + 2.f / NNP_PI_F * atanf(zz));
+        d = 0.5f * (1.f + z / (1.f + zz * zz)) + 1.f / NNP_PI_F * atanf(zz);
+    } break;
+    case NEU_IERF: {            // the reference uses the A&S 7.1.26 erf approximation
+        const float fexp = expf(-z * z);
+        const float zs = (float)((0.f < z) - (z < 0.f));
+        const float t = 1.f / (1.f + 0.3275911f * z * zs);
+        const float ferf = zs * (1.f - t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f)))) * fexp);
+        a = 0.5f * (z * ferf + (fexp + z * NNP_RADPI_F - 1.f) / NNP_RADPI_F);
+        d = 0.5f * (ferf + 1.f);
+    } break;
+    case NEU_TEST: {
+        const float zz = c * z, z2 = zz * zz, z4 = z2 * z2, den = rsqrtf(sqrtf(z4 + 1.f));
+        a = 0.5f * z * (1.f + zz * den);
+        d = 0.5f * (zz * den * (1.f + 1.f / (z4 + 1.f)) + 1.f);
+    } break;
+    default: a = 0.f; d = 0.f;
+    }
+}
+
+// ---------------------------------------------------------------- warp helpers
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(NNP_FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(NNP_FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ bool finite_d(double x) { return fabs(x) <= 1.7976931348623157e308; }
+
+// accumulate a pair term: FP32 fused multiply-add, or the FP32 product added in FP64
+__device__ __forceinline__ void acc_add(float &acc, float a, float b) { acc = fmaf(a, b, acc); }
+__device__ __forceinline__ void acc_add(double &acc, float a, float b) { acc += (double)(a * b); }
+
+// ---------------------------------------------------------------- per-atom staging
+
+// Per-warp shared-memory view of one atom's neighbours.
+struct NbrView {
+    float4 *u;          // unit vector to the neighbour and inverse distance (ux, uy, uz, 1/r) [C]
+    float *r;           // distance [C]
+    float4 *par;        // block parameters [NNP_MAX_AFUNC]
+    int *j;             // neighbour atom index [C]
+    float *fc, *fd;     // cutoff value / slope [ncut][C]
+    float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr [ndamp][C]
+    float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
+    float *vec;         // dE/dG row [gstride]
+    float *pc;          // pair coefficients [4][NNP_PCH]
+    int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
+    unsigned char *t;   // neighbour type [C]
+};
+
+NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
+{
+    return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 2 * ndamp * C +
+           (force ? 3 * C + gstride + 4 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+}
+
+__device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
+{
+    NbrView v;
+    float *p = base;
+    v.u = reinterpret_cast<float4 *>(p); p += 4 * C;                 // 16-byte aligned first
+    v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
+    v.r = p; p += C;
+    v.j = reinterpret_cast<int *>(p); p += C;
+    v.fc = p; p += ncut * C;
+    v.fd = p; p += ncut * C;
+    v.w = p; p += ndamp * C;
+    v.wd = p; p += ndamp * C;
+    if (force) {
+        v.gx = p; p += C;
+        v.gy = p; p += C;
+        v.gz = p; p += C;
+        v.vec = p; p += gstride;
+        v.pc = p; p += 4 * NNP_PCH;
+    } else {
+        v.gx = v.gy = v.gz = v.vec = v.pc = nullptr;
+    }
+    v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
+    v.t = reinterpret_cast<unsigned char *>(p);
+    return v;
+}
+
+// Load atom i's neighbour list into the warp's view and compute the per-neighbour
+// quantities: unit vector, distance, cutoff value/slope per cutoff, and the
+// GAUSS damping factors w_e(r) = fc(r) exp(-a_e r^2) with slopes dw_e/dr.
+__device__ inline int stage_neighbors(const NbrView &v, i64 i, int cap, const float4 *__restrict__ nbr,
+                                      const int *__restrict__ nbr_cnt, const DevPot &P, const DevType &T, int lane)
+{
+    const int n = nbr_cnt[i];
+    for (int k = lane; k < n; k += 32) {
+        const float4 e = nbr[i * cap + k];
+        const float r = sqrtf(e.x * e.x + e.y * e.y + e.z * e.z);
+        const float ir = 1.f / r;
+        v.u[k] = make_float4(e.x * ir, e.y * ir, e.z * ir, ir);
+        v.r[k] = r;
+        const int pk = __float_as_int(e.w);
+        v.j[k] = pk & 0x0fffffff;
+        v.t[k] = (unsigned char)((unsigned)pk >> 28);
+        for (int c = 0; c < P.ncut; ++c) {
+            float f, g;
+            cutoff_fg(P.cut[c], r, f, g);
+            v.fc[c * cap + k] = f;
+            v.fd[c * cap + k] = g;
+        }
+        for (int d = 0; d < T.ndamp; ++d) {
+            const int c = T.damp_cut[d];
+            const float a = T.damp_a[d];
+            const float ex = expf(-a * r * r);
+            const float f = v.fc[c * cap + k], g = v.fd[c * cap + k];
+            v.w[d * cap + k] = f * ex;
+            v.wd[d * cap + k] = (g - 2.f * a * r * f) * ex;
+        }
+    }
+    // type segment starts (the list is grouped by type)
+    for (int t = 0; t <= P.ntypes; ++t) {
+        int c = 0;
+        for (int kb = 0; kb < n; kb += 32) {
+            const int k = kb + lane;
+            c += __popc(__ballot_sync(NNP_FULL, k < n && v.t[k] < t));
+        }
+        if (lane == 0) v.seg[t] = c;
+    }
+    __syncwarp();
+    return n;
+}
+
+__device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
+{
+    K = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
+    while (K * (K + 1) / 2 > tt) --K;
+    while ((K + 1) * (K + 2) / 2 <= tt) ++K;
+    J = tt - K * (K + 1) / 2;
+}
+
+// One angular block as seen by a warp: segments of the two neighbour types and
+// the numbering of its pairs, p = g*m + f with a fast index f in [0,m):
+//  - J != K (rectangle): m = nb, pair (a,b) = (g, f);
+//  - J == K (fold):      m = n,  pair (a,b) = (f, (f+g+1) mod n) for
+//    g < (n-1)/2, and for even n a last half row g = n/2-1, f < n/2.
+//    Every unordered pair of distinct slots appears exactly once:
+//    n*floor((n-1)/2) + (n even ? n/2 : 0) = n(n-1)/2 pairs.
+// Lanes step p by 32, which is (q32, r32) = (32/m, 32%m) in (g, f): two
+// adds and one wrap per step instead of a division or a square root.
+struct Blk {
+    int sa, na;       // first member: segment start / size
+    int sb, nb;       // second member (sb == sa for J == K)
+    bool tri;
+    int npairs;
+    int m, q32, r32;
+};
+
+__device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
+{
+    k.sa = v.seg[J];
+    k.na = v.seg[J + 1] - k.sa;
+    k.tri = (J == K);
+    k.sb = k.tri ? k.sa : v.seg[K];
+    k.nb = k.tri ? k.na : v.seg[K + 1] - v.seg[K];
+    k.npairs = k.tri ? k.na * (k.na - 1) / 2 : k.na * k.nb;
+    if (k.npairs == 0) return false;
+    k.m = k.nb;
+    k.q32 = 32 / k.m;
+    k.r32 = 32 - k.q32 * k.m;
+    return true;
+}
+
+struct PairIt {
+    int f, g;
+};
+
+__device__ __forceinline__ PairIt pit_init(const Blk &k, int p)
+{
+    PairIt it;
+    it.g = p / k.m;
+    it.f = p - it.g * k.m;
+    return it;
+}
+
+__device__ __forceinline__ void pit_next(const Blk &k, PairIt &it)
+{
+    it.f += k.r32;
+    it.g += k.q32;
+    if (it.f >= k.m) {
+        it.f -= k.m;
+        ++it.g;
+    }
+}
+
+// neighbour slots (a, b) of the pair at `it`
+__device__ __forceinline__ void pit_slots(const Blk &k, const PairIt &it, int &a, int &b)
+{
+    if (k.tri) {
+        const int bb = it.f + it.g + 1;
+        a = k.sa + it.f;
+        b = k.sa + (bb >= k.m ? bb - k.m : bb);
+    } else {
+        a = k.sa + it.g;
+        b = k.sb + it.f;
+    }
+}
+
+// ---------------------------------------------------------------- generic block code
+
+// Symmetry functions of one angular block, parameters from v.par (any form).
+template <typename Acc>
+__device__ void symm_block_generic(const NbrView &v, const DevBlockA &B, const Blk &k, int cap, int lane, float *Gi)
+{
+    if (B.form == ANG_GAUSS) {
+        // damping exp(-(ra^2+rb^2)/eta^2) fc(ra) fc(rb) = w(ra) w(rb) from the
+        // staged factors; NNP_SYMM_CHUNK functions per pass in registers
+        for (int f0 = 0; f0 < B.n; f0 += NNP_SYMM_CHUNK) {
+            const int nf = min(NNP_SYMM_CHUNK, B.n - f0);
+            Acc acc[NNP_SYMM_CHUNK];
+#pragma unroll
+            for (int f = 0; f < NNP_SYMM_CHUNK; ++f) acc[f] = 0;
+            PairIt it = pit_init(k, lane);
+#pragma unroll 1
+            for (int p = lane; p < k.npairs; p += 32, pit_next(k, it)) {
+                int a, b;
+                pit_slots(k, it, a, b);
+                const float4 ua = v.u[a], ub = v.u[b];
+                const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+                int dcur = -1;
+                float damp = 0.f;
+#pragma unroll
+                for (int f = 0; f < NNP_SYMM_CHUNK; ++f) {
+                    if (f < nf) {
+                        const float4 q = v.par[f0 + f];
+                        const int pk = __float_as_int(q.w);
+                        const int d = pk & 0xff, iz = (pk >> 8) - 1;
+                        if (d != dcur) {
+                            dcur = d;
+                            damp = v.w[d * cap + a] * v.w[d * cap + b];
+                        }
+                        float pz, pm1;
+                        ang_pow(cs, q.x, q.y, iz, pz, pm1);
+                        acc_add(acc[f], pz, damp);
+                    }
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < NNP_SYMM_CHUNK; ++f) {
+                if (f < nf) {
+                    const Acc s = warp_sum(acc[f]);
+                    if (lane == 0) Gi[B.off_g + f0 + f] = (float)s;
+                }
+            }
+        }
+    } else {
+        // other forms: one function per pass over the pairs
+        for (int f = 0; f < B.n; ++f) {
+            const float4 q = v.par[f];
+            const int iz = (__float_as_int(q.w) >> 8) - 1;
+            Acc acc = 0;
+            PairIt it = pit_init(k, lane);
+#pragma unroll 1
+            for (int p = lane; p < k.npairs; p += 32, pit_next(k, it)) {
+                int a, b;
+                pit_slots(k, it, a, b);
+                const float4 ua = v.u[a], ub = v.u[b];
+                const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+                float h, hc, hrj, hrk;
+                angular_generic(B.form, v.r[a], v.r[b], cs, v.fc[B.cut * cap + a], v.fc[B.cut * cap + b], 0.f, 0.f, q.x,
+                                q.y, iz, q.z, false, h, hc, hrj, hrk);
+                acc_add(acc, h, 1.f);
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) Gi[B.off_g + f] = (float)acc;
+        }
+    }
+}
+
+// Writes the four dE/dd coefficients of one pair (see force_body); ira, irb
+// are the inverse distances.
+__device__ __forceinline__ void pair_coeffs(float *pc, int q, float hc, float hra, float hrb, float cs, float ira,
+                                            float irb)
+{
+    pc[q] = hra - hc * cs * ira;                 // on u_a in dE/dd_a
+    pc[NNP_PCH + q] = hc * ira;                  // on u_b in dE/dd_a
+    pc[2 * NNP_PCH + q] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
+    pc[3 * NNP_PCH + q] = hc * irb;              // on u_a in dE/dd_b
+}
+
+// Pair pass of the force kernel for pairs [c0,c1) of one block (any form):
+// dE/dcos, dE/dr_a, dE/dr_b from e = dE/dG of the block's functions.
+__device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B, const Blk &k, int c0, int c1, int cap,
+                                    int lane)
+{
+    const float *eb = v.vec + B.off_g;
+    const bool gauss = (B.form == ANG_GAUSS);
+    PairIt it = pit_init(k, c0 + lane);
+#pragma unroll 1
+    for (int p = c0 + lane; p < c1; p += 32, pit_next(k, it)) {
+        int a, b;
+        pit_slots(k, it, a, b);
+        const float4 ua = v.u[a], ub = v.u[b];
+        const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+        float hc = 0.f, hra = 0.f, hrb = 0.f;
+        if (gauss) {
+            int dcur = -1;
+            float sc = 0.f, sp = 0.f;
+            for (int f = 0; f < B.n; ++f) {
+                const float4 q = v.par[f];
+                const int pk = __float_as_int(q.w);
+                const int d = pk & 0xff, iz = (pk >> 8) - 1;
+                if (d != dcur) {
+                    if (dcur >= 0) {
+                        const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                        hc = fmaf(sc, wa * wb, hc);
+                        hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
+                        hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
+                    }
+                    dcur = d;
+                    sc = 0.f;
+                    sp = 0.f;
+                }
+                float pz, pm1;
+                ang_pow(cs, q.x, q.y, iz, pz, pm1);
+                const float ef = eb[f];
+                sc = fmaf(ef * q.y * q.x, pm1, sc);
+                sp = fmaf(ef, pz, sp);
+            }
+            if (dcur >= 0) {
+                const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                hc = fmaf(sc, wa * wb, hc);
+                hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
+                hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
+            }
+        } else {
+            const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];
+            const float ga = v.fd[B.cut * cap + a], gb = v.fd[B.cut * cap + b];
+            for (int f = 0; f < B.n; ++f) {
+                const float4 q = v.par[f];
+                const int iz = (__float_as_int(q.w) >> 8) - 1;
+                float h, dc, dra, drb;
+                angular_generic(B.form, v.r[a], v.r[b], cs, ca, cb, ga, gb, q.x, q.y, iz, q.z, true, h, dc, dra, drb);
+                const float ef = eb[f];
+                hc = fmaf(ef, dc, hc);
+                hra = fmaf(ef, dra, hra);
+                hrb = fmaf(ef, drb, hrb);
+            }
+        }
+        pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);
+    }
+}
+
+// Slot pass: each lane owns neighbour slots of the block and sums, in a fixed
+// order, the coefficients of the pairs [c0,c1) that contain them.  With the
+// numbering of Blk, slot x of a J == K block is the first member of the pairs
+// (x, x+s mod n) at p = (s-1)n + x and the second member of the pairs
+// (x-s mod n, x) at p = (s-1)n + (x-s mod n), s = 1..(n-1)/2, plus s = n/2
+// for even n (first member if x < n/2, second member otherwise).
+__device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c1, int lane)
+{
+    const float *cA = v.pc, *cB = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH, *cD = v.pc + 3 * NNP_PCH;
+    if (k.tri) {
+        const int n = k.m, h = (n - 1) >> 1;
+        const int gmin = c0 / n, gmax = min((c1 - 1) / n, (n >> 1) - 1);   // rows g = s-1 touching the chunk
+        for (int x = lane; x < n; x += 32) {
+            const int slot = k.sa + x;
+            const float4 us = v.u[slot];
+            float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+            for (int g = gmin; g <= gmax; ++g) {
+                const bool last = (g == h);                  // even n: half row
+                // first member: partner x+g+1
+                if (!last || x < (n >> 1)) {
+                    const int p = g * n + x;
+                    if (p >= c0 && p < c1) {
+                        int b = x + g + 1;
+                        b = (b >= n) ? b - n : b;
+                        const float4 ub = v.u[k.sa + b];
+                        sa_ += cA[p - c0];
+                        const float bt = cB[p - c0];
+                        vx = fmaf(bt, ub.x, vx);
+                        vy = fmaf(bt, ub.y, vy);
+                        vz = fmaf(bt, ub.z, vz);
+                    }
+                }
+                // second member: partner y = x-g-1 (mod n)
+                if (!last || x >= (n >> 1)) {
+                    int y = x - g - 1;
+                    y = (y < 0) ? y + n : y;
+                    const int p = g * n + y;
+                    if (p >= c0 && p < c1) {
+                        const float4 ua = v.u[k.sa + y];
+                        sa_ += cC[p - c0];
+                        const float dt = cD[p - c0];
+                        vx = fmaf(dt, ua.x, vx);
+                        vy = fmaf(dt, ua.y, vy);
+                        vz = fmaf(dt, ua.z, vz);
+                    }
+                }
+            }
+            v.gx[slot] += fmaf(sa_, us.x, vx);
+            v.gy[slot] += fmaf(sa_, us.y, vy);
+            v.gz[slot] += fmaf(sa_, us.z, vz);
+        }
+        return;
+    }
+    const int nslots = k.na + k.nb;
+    for (int sl = lane; sl < nslots; sl += 32) {
+        const bool is_row = sl < k.na;                 // first member of its pairs
+        const int slot = is_row ? k.sa + sl : k.sb + (sl - k.na);
+        const float4 us = v.u[slot];
+        float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+        if (is_row) {
+            const int rs = sl * k.nb;
+            const int p0 = max(rs, c0), p1 = min(rs + k.nb, c1);
+            for (int p = p0; p < p1; ++p) {
+                const float4 ub = v.u[k.sb + (p - rs)];
+                sa_ += cA[p - c0];
+                const float bt = cB[p - c0];
+                vx = fmaf(bt, ub.x, vx);
+                vy = fmaf(bt, ub.y, vy);
+                vz = fmaf(bt, ub.z, vz);
+            }
+        } else {
+            const int ic = sl - k.na;
+            // rows ra with c0 <= ra*nb + ic < c1 (c0 - ic > -nb, so the first quotient rounds up)
+            const int a0 = (c0 - ic + k.nb - 1) / k.nb;
+            const int a1 = (c1 - 1 - ic >= 0) ? min(k.na, (c1 - 1 - ic) / k.nb + 1) : 0;
+            for (int ra = a0; ra < a1; ++ra) {
+                const int p = ra * k.nb + ic;
+                const float4 ua = v.u[k.sa + ra];
+                sa_ += cC[p - c0];
+                const float dt = cD[p - c0];
+                vx = fmaf(dt, ua.x, vx);
+                vy = fmaf(dt, ua.y, vy);
+                vz = fmaf(dt, ua.z, vz);
+            }
+        }
+        v.gx[slot] += fmaf(sa_, us.x, vx);
+        v.gy[slot] += fmaf(sa_, us.y, vy);
+        v.gz[slot] += fmaf(sa_, us.z, vz);
+    }
+}
+
+// Prebuilt path: every angular block goes through the generic code above.
+struct GenericBlocks {
+    template <typename Acc>
+    // Gb: the block's first symmetry function in the atom's row; eb: its first dE/dG
+    __device__ static bool symm(const NbrView &, int, int, const Blk &, int, int, float *) { return false; }
+    __device__ static bool force(const NbrView &, int, int, const Blk &, int, int, int, int, const float *)
+    {
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------- kernel bodies
+
+// Symmetry functions of atoms [warp-strided]: NNP::compute_symm (nnp/nnp.cpp:350-392).
+// Radial: lanes own functions and walk their neighbour-type segment.  Angular:
+// one (J,K) block at a time, lanes over the block's pairs.  Blocks::symm may
+// take over a block with code specialised for it.
+// Atoms are visited in `order` (grouped by element), so at any time the SMs
+// run one element's block code, which keeps the instruction working set small.
+template <typename Acc, class Blocks>
+__device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *__restrict__ rpar,
+                          const float4 *__restrict__ apar, const int *__restrict__ type, const int *__restrict__ order,
+                          const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, int ncut_max,
+                          int ndamp_max, int gstride, float *__restrict__ G, float *smem)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, false);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, false);
+    const DevPot &P = *pot;
+    for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
+        const i64 i = order[idx];
+        const int II = type[i];
+        const DevType &T = P.t[II];
+        stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        float *Gi = G + i * gstride;
+        for (int g = lane; g < gstride; g += 32) Gi[g] = 0.f;
+        __syncwarp();
+        for (int J = 0; J < P.ntypes; ++J) {
+            const DevBlockR B = T.br[J];
+            if (B.n == 0) continue;
+            const int s0 = v.seg[J], s1 = v.seg[J + 1];
+            for (int f = lane; f < B.n; f += 32) {
+                const float2 q = rpar[B.par + f];
+                Acc acc = 0;
+                for (int k = s0; k < s1; ++k) {
+                    float val, der;
+                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
+                    acc_add(acc, val, 1.f);
+                }
+                Gi[B.off_g + f] = (float)acc;
+            }
+        }
+        const int TT = P.ntypes * (P.ntypes + 1) / 2;
+        for (int tt = 0; tt < TT; ++tt) {
+            const DevBlockA B = T.ba[tt];
+            if (B.n == 0) continue;
+            int J, K;
+            tt_decode(tt, J, K);
+            Blk k;
+            if (!make_blk(v, J, K, k)) continue;
+            if (!Blocks::template symm<Acc>(v, II, tt, k, cap, lane, Gi + B.off_g)) {
+                for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
+                __syncwarp();
+                symm_block_generic<Acc>(v, B, k, cap, lane, Gi);
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+    }
+}
+
+// Forces: NNP::compute_force (nnp/nnp.cpp:412-476).  With e = dE_i/dG_i, every
+// pair and triplet contributes dE_i/dd_j for the neighbour displacements
+// d_j = x_i - x_j - R q.  For a triplet (a,b) with dE/dcos = hc,
+// dE/dr_a = hra, dE/dr_b = hrb:
+//   dE/dd_a = (hra - hc cos/r_a) u_a + (hc/r_a) u_b,  and a <-> b.
+// The pair pass writes these four coefficients per pair into shared memory,
+// then each lane owns neighbour slots and sums their pairs in a fixed order
+// (no atomics).  Finally F_j += g_j and F_i -= sum_j g_j in FP64: the
+// Newton-3 scatter of nnp.cpp:443-471.
+template <class Blocks>
+__device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *__restrict__ rpar,
+                           const float4 *__restrict__ apar, const int *__restrict__ type, const int *__restrict__ order,
+                           const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, int ncut_max,
+                           int ndamp_max, int gstride, const float *__restrict__ dEdG, double *__restrict__ F,
+                           DevErr *err, float *smem)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
+    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
+    const DevPot &P = *pot;
+    for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
+        const i64 i = order[idx];
+        const int II = type[i];
+        const DevType &T = P.t[II];
+        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        const float *e = dEdG + i * gstride;
+        for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
+        __syncwarp();
+        // radial: lanes own their neighbour slot (initialises g)
+        for (int k = lane; k < n; k += 32) {
+            const DevBlockR B = T.br[v.t[k]];
+            const float4 u = v.u[k];
+            const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
+            float amp = 0.f;
+            for (int f = 0; f < B.n; ++f) {
+                const float2 q = rpar[B.par + f];
+                float val, der;
+                radial_fd(B.form, v.r[k], q.x, q.y, fc, fd, val, der);
+                amp = fmaf(v.vec[B.off_g + f], der, amp);
+            }
+            v.gx[k] = amp * u.x;
+            v.gy[k] = amp * u.y;
+            v.gz[k] = amp * u.z;
+        }
+        __syncwarp();
+        const int TT = P.ntypes * (P.ntypes + 1) / 2;
+        for (int tt = 0; tt < TT; ++tt) {
+            const DevBlockA B = T.ba[tt];
+            if (B.n == 0) continue;
+            int J, K;
+            tt_decode(tt, J, K);
+            Blk k;
+            if (!make_blk(v, J, K, k)) continue;
+            bool staged = false;
+            for (int c0 = 0; c0 < k.npairs; c0 += NNP_PCH) {
+                const int c1 = min(k.npairs, c0 + NNP_PCH);
+                if (!Blocks::force(v, II, tt, k, c0, c1, cap, lane, v.vec + B.off_g)) {
+                    if (!staged) {
+                        for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
+                        __syncwarp();
+                        staged = true;
+                    }
+                    force_pairs_generic(v, B, k, c0, c1, cap, lane);
+                }
+                __syncwarp();
+                force_slots(v, k, c0, c1, lane);
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+        // scatter: F_j += g_j, F_i -= sum g_j
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        bool bad = false;
+        for (int k = lane; k < n; k += 32) {
+            const double gx = v.gx[k], gy = v.gy[k], gz = v.gz[k];
+            bad |= !(finite_d(gx) && finite_d(gy) && finite_d(gz));
+            const i64 j = v.j[k];
+            atomicAdd(&F[3 * j], gx);
+            atomicAdd(&F[3 * j + 1], gy);
+            atomicAdd(&F[3 * j + 2], gz);
+            fx += gx;
+            fy += gy;
+            fz += gz;
+        }
+        fx = warp_sum(fx);
+        fy = warp_sum(fy);
+        fz = warp_sum(fz);
+        if (lane == 0) {
+            atomicAdd(&F[3 * i], -fx);
+            atomicAdd(&F[3 * i + 1], -fy);
+            atomicAdd(&F[3 * i + 2], -fz);
+        }
+        if (__any_sync(NNP_FULL, bad) && lane == 0) atomicMax(&err->nonfinite, 1);
+        __syncwarp();
+    }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace nnp

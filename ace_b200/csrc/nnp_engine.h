@@ -23,14 +23,6 @@ struct StructGrid {
     int pbc;
 };
 
-// device error record: kernels raise flags, the host reads them after a step
-struct DevErr {
-    int need_cap;     // largest neighbour count seen (when above the capacity)
-    int bad_type;     // an atom type was outside [0, ntypes)
-    int bad_cell;     // a periodic cell had no volume
-    int nonfinite;    // a non-finite energy or force
-};
-
 template <class T>
 struct DBuf {
     T *p = nullptr;
@@ -66,6 +58,17 @@ struct Engine {
     int64_t wfloats = 0;
     int gstride = 0;              // row length of G / dE/dG (max n_input rounded up to 4)
     int precision = 0;
+    bool acc64 = false;           // FP64 running sums of the symmetry functions
+    std::vector<float2> rpar_host;
+    std::vector<float4> apar_host;
+    std::vector<float> wpar_host;
+    std::vector<double> vac_host;
+
+    // kernels specialised for this potential at run time (nnp_jit.cpp)
+    bool use_jit = true;
+    void *jit_module = nullptr;   // cudaLibrary_t
+    void *jit_symm = nullptr, *jit_force = nullptr;   // cudaKernel_t
+    std::string jit_source, jit_error;
 
     // stream / events
     cudaStream_t stream = nullptr;
@@ -82,6 +85,8 @@ struct Engine {
     DBuf<StructGrid> grid;
     DBuf<int> cell_cnt, cell_start, cell_fill, cell_atoms, scan_tmp;
     DBuf<double4> cell_pos;       // cell-ordered wrapped positions, type in .w
+    DBuf<int> order;              // atoms grouped by element (visiting order of the per-atom kernels)
+    DBuf<int> type_fill;          // [2 * NNP_MAX_TYPES] element counts and fill cursors
     DBuf<float4> nbr;
     DBuf<int> nbr_cnt;
     DBuf<float> G, dEdG, e_atom;
@@ -103,7 +108,8 @@ struct Engine {
         if (timing && ev[k]) cudaEventRecord(ev[k], stream);
     }
 
-    // build the device potential from `host`
+    // device tables of the potential from `host` (host-side only), and their upload
+    std::string build_tables();
     std::string upload();
     void free_all();
 };
@@ -118,5 +124,12 @@ std::string run_energy(Engine &E, bool vacuum);
 std::string run_symm_to_double(Engine &E, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
+
+// run-time specialised kernels (nnp_jit.cpp)
+std::string jit_compile(const Engine &E, std::string &source, std::vector<char> &cubin);
+std::string jit_build(Engine &E);
+std::string &jit_last_log();   // compiler messages of the last NVRTC compilation
+void jit_release(Engine &E);
+std::string jit_launch(void *fn, int grid, int block, size_t smem, cudaStream_t stream, void **args);
 
 }  // namespace nnp

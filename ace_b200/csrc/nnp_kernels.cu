@@ -20,29 +20,13 @@
 //   k_energy       one block per structure, FP64 energy sum
 #include <cstdio>
 
+#include "nnp_device.cuh"
 #include "nnp_engine.h"
-#include "nnp_math.cuh"
 
 namespace nnp {
 
-#define FULL 0xffffffffu
-#define WARPS 8
-#define SYMM_CHUNK 8   // angular functions accumulated in registers per pass
-#define SYMM_CHUNK 8   // angular functions accumulated in registers per pass
-
-__device__ __forceinline__ float warp_sum(float v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
-
-__device__ __forceinline__ double warp_sum_d(double v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
+#define FULL NNP_FULL
+#define WARPS NNP_WARPS
 
 __device__ __forceinline__ int floor_div(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
 
@@ -77,6 +61,45 @@ __global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N,
     atom_struct[i] = lo;
     const int t = type[i];
     if (t < 0 || t >= ntypes) atomicMax(&err->bad_type, 1);
+}
+
+// Atoms grouped by element: per-block counts in shared memory, one global
+// atomic per (block, element) to count, then one to reserve each block's range.
+__global__ void k_type_count(int64_t N, const int *__restrict__ type, int ntypes, int *__restrict__ cnt)
+{
+    __shared__ int c[NNP_MAX_TYPES];
+    if (threadIdx.x < NNP_MAX_TYPES) c[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < N) {
+        const int t = type[i];
+        if (t >= 0 && t < ntypes) atomicAdd(&c[t], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < ntypes && c[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], c[threadIdx.x]);
+}
+
+__global__ void k_type_scatter(int64_t N, const int *__restrict__ type, int ntypes, const int *__restrict__ cnt,
+                               int *__restrict__ fill, int *__restrict__ order)
+{
+    __shared__ int c[NNP_MAX_TYPES], base[NNP_MAX_TYPES];
+    if (threadIdx.x < NNP_MAX_TYPES) c[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int t = -1, r = 0;
+    if (i < N) {
+        t = type[i];
+        if (t >= 0 && t < ntypes) r = atomicAdd(&c[t], 1);
+        else t = -1;
+    }
+    __syncthreads();
+    if (threadIdx.x < ntypes) {
+        int start = 0;
+        for (int k = 0; k < (int)threadIdx.x; ++k) start += cnt[k];
+        base[threadIdx.x] = start + (c[threadIdx.x] ? atomicAdd(&fill[threadIdx.x], c[threadIdx.x]) : 0);
+    }
+    __syncthreads();
+    if (t >= 0) order[base[t] + r] = (int)i;
 }
 
 __global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *__restrict__ off, int S, int pbc,
@@ -363,286 +386,21 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_neigh(int64_t N, const int *_
     }
 }
 
-// ------------------------------------------------------------------ per-atom staging
-
-// Per-warp shared-memory view of one atom's neighbours.
-struct NbrView {
-    float4 *u;          // unit vector to the neighbour and distance (ux, uy, uz, r) [C]
-    float4 *par;        // block parameters [NNP_MAX_AFUNC]
-    int *j;             // neighbour atom index [C]
-    float *fc, *fd;     // cutoff value / slope [ncut][C]
-    float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr [ndamp][C]
-    float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
-    float *vec;         // dE/dG row [gstride]
-    float *pc;          // pair coefficients [4][PCH]
-    int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
-    unsigned char *t;   // neighbour type [C]
-};
-
-#define PCH 256         // pairs per force chunk
-
-__host__ __device__ inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
-{
-    return 4 * C + 4 * NNP_MAX_AFUNC + C + 2 * ncut * C + 2 * ndamp * C + (force ? 3 * C + gstride + 4 * PCH : 0) +
-           NNP_MAX_TYPES + 1 + (C + 3) / 4;
-}
-
-__device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
-{
-    NbrView v;
-    float *p = base;
-    v.u = reinterpret_cast<float4 *>(p); p += 4 * C;                 // 16-byte aligned first
-    v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
-    v.j = reinterpret_cast<int *>(p); p += C;
-    v.fc = p; p += ncut * C;
-    v.fd = p; p += ncut * C;
-    v.w = p; p += ndamp * C;
-    v.wd = p; p += ndamp * C;
-    if (force) {
-        v.gx = p; p += C;
-        v.gy = p; p += C;
-        v.gz = p; p += C;
-        v.vec = p; p += gstride;
-        v.pc = p; p += 4 * PCH;
-    } else {
-        v.gx = v.gy = v.gz = v.vec = v.pc = nullptr;
-    }
-    v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
-    v.t = reinterpret_cast<unsigned char *>(p);
-    return v;
-}
-
-// Load atom i's neighbour list into the warp's view and compute the per-neighbour
-// quantities: unit vector, distance, cutoff value/slope per cutoff, and the
-// GAUSS damping factors w_e(r) = fc(r) exp(-a_e r^2) with slopes dw_e/dr.
-__device__ inline int stage_neighbors(const NbrView &v, int64_t i, int cap, const float4 *__restrict__ nbr,
-                                      const int *__restrict__ nbr_cnt, const DevPot &P, const DevType &T, int lane)
-{
-    const int n = nbr_cnt[i];
-    for (int k = lane; k < n; k += 32) {
-        const float4 e = nbr[i * cap + k];
-        const float r = sqrtf(e.x * e.x + e.y * e.y + e.z * e.z);
-        const float ir = 1.f / r;
-        v.u[k] = make_float4(e.x * ir, e.y * ir, e.z * ir, r);
-        const int pk = __float_as_int(e.w);
-        v.j[k] = pk & 0x0fffffff;
-        v.t[k] = (unsigned char)((unsigned)pk >> 28);
-        for (int c = 0; c < P.ncut; ++c) {
-            float f, g;
-            cutoff_fg(P.cut[c], r, f, g);
-            v.fc[c * cap + k] = f;
-            v.fd[c * cap + k] = g;
-        }
-        for (int d = 0; d < T.ndamp; ++d) {
-            const int c = T.damp_cut[d];
-            const float a = T.damp_a[d];
-            const float ex = expf(-a * r * r);
-            const float f = v.fc[c * cap + k], g = v.fd[c * cap + k];
-            v.w[d * cap + k] = f * ex;
-            v.wd[d * cap + k] = (g - 2.f * a * r * f) * ex;
-        }
-    }
-    // type segment starts (the list is grouped by type)
-    for (int t = 0; t <= P.ntypes; ++t) {
-        int c = 0;
-        for (int kb = 0; kb < n; kb += 32) {
-            const int k = kb + lane;
-            c += __popc(__ballot_sync(FULL, k < n && v.t[k] < t));
-        }
-        if (lane == 0) v.seg[t] = c;
-    }
-    __syncwarp();
-    return n;
-}
-
-// Pairs of one (J,K) block, segment-local: rectangle a in [0,na) x b in [0,nb)
-// (J != K, index p = a*nb + b) or lower triangle b < a < na (J == K,
-// p = a(a-1)/2 + b).
-__device__ __forceinline__ int tri_row(int p)
-{
-    int r = (int)((1.f + sqrtf(8.f * (float)p + 1.f)) * 0.5f);
-    if (r * (r - 1) / 2 > p) --r;
-    else if ((r + 1) * r / 2 <= p) ++r;
-    return r;
-}
-
-__device__ __forceinline__ void pair_at(bool tri, int nb, int p, int &a, int &b)
-{
-    if (tri) {
-        a = tri_row(p);
-        b = p - a * (a - 1) / 2;
-    } else {
-        a = p / nb;
-        b = p - a * nb;
-    }
-}
-
-__device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
-{
-    K = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
-    while (K * (K + 1) / 2 > tt) --K;
-    while ((K + 1) * (K + 2) / 2 <= tt) ++K;
-    J = tt - K * (K + 1) / 2;
-}
-
-// x^n, 0 <= n < 64, by binary powering with branches on the (warp-uniform) bits of n
-__device__ __forceinline__ float upow(float x, int n)
-{
-    float r = (n & 1) ? x : 1.f;
-    if (n >> 1) {
-        x *= x;
-        if (n & 2) r *= x;
-        if (n >> 2) {
-            x *= x;
-            if (n & 4) r *= x;
-            if (n >> 3) {
-                x *= x;
-                if (n & 8) r *= x;
-                if (n >> 4) {
-                    x *= x;
-                    if (n & 16) r *= x;
-                    if (n >> 5) { x *= x; r *= x; }
-                }
-            }
-        }
-    }
-    return r;
-}
-
-// (0.5 + lf cos)^zeta and (.)^(zeta-1), reference form |0.5 + lambda/2 cos|^zeta
-__device__ __forceinline__ void ang_pow(float cs, float lf, float zeta, int iz, float &pz, float &pm1)
-{
-    const float x = fabsf(fmaf(lf, cs, 0.5f));
-    if (iz > 0) {
-        pm1 = upow(x, iz - 1);
-        pz = pm1 * x;
-    } else if (iz == 0) {
-        pm1 = 0.f;
-        pz = 1.f;
-    } else {
-        pm1 = (x > 0.f) ? exp2f((zeta - 1.f) * log2f(x)) : 0.f;
-        pz = pm1 * x;
-    }
-}
-
 // ------------------------------------------------------------------ symmetry functions
 
+// Acc is the type of the per-lane running sums: each lane adds up to T/32 pair
+// terms of one function, so FP32 sums lose ~sqrt(T/32) ulps; FP64 sums keep G
+// to the FP32 rounding of the final value.
+template <typename Acc>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot *__restrict__ pot,
                                                        const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
-                                                       const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                       const int *__restrict__ type, const int *__restrict__ order, const float4 *__restrict__ nbr,
                                                        const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
                                                        int gstride, float *__restrict__ G)
 {
     extern __shared__ float4 smem4[];
-    float *smem = reinterpret_cast<float *>(smem4);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, false);
-    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, false);
-    const DevPot &P = *pot;
-    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
-        const int II = type[i];
-        const DevType &T = P.t[II];
-        stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
-        float *Gi = G + i * gstride;
-        for (int g = lane; g < gstride; g += 32) Gi[g] = 0.f;
-        __syncwarp();
-        // ---- radial: one block per neighbour type; lanes own functions and
-        // walk that type's neighbour segment (no cross-lane reduction)
-        for (int J = 0; J < P.ntypes; ++J) {
-            const DevBlockR B = T.br[J];
-            if (B.n == 0) continue;
-            const int s0 = v.seg[J], s1 = v.seg[J + 1];
-            for (int f = lane; f < B.n; f += 32) {
-                const float2 q = rpar[B.par + f];
-                float acc = 0.f;
-                for (int k = s0; k < s1; ++k) {
-                    float val, der;
-                    radial_fd(B.form, v.u[k].w, q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
-                    acc += val;
-                }
-                Gi[B.off_g + f] = acc;
-            }
-        }
-        // ---- angular: one block per neighbour-type pair J <= K, lanes over pairs
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
-            const DevBlockA B = T.ba[tt];
-            if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
-            const int sa = v.seg[J], na = v.seg[J + 1] - sa;
-            const int sb = v.seg[K], nb = v.seg[K + 1] - sb;
-            const bool tri = (J == K);
-            const int npairs = tri ? na * (na - 1) / 2 : na * nb;
-            if (npairs == 0) continue;
-            const int sB = tri ? sa : sb;
-            for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
-            __syncwarp();
-            if (B.form == ANG_GAUSS) {
-                // damping exp(-(ra^2+rb^2)/eta^2) fc(ra) fc(rb) = w(ra) w(rb) from the
-                // staged factors; SYMM_CHUNK functions per pass in registers
-                for (int f0 = 0; f0 < B.n; f0 += SYMM_CHUNK) {
-                    const int nf = min(SYMM_CHUNK, B.n - f0);
-                    float acc[SYMM_CHUNK];
-#pragma unroll
-                    for (int f = 0; f < SYMM_CHUNK; ++f) acc[f] = 0.f;
-                    for (int p = lane; p < npairs; p += 32) {
-                        int ia, ib;
-                        pair_at(tri, nb, p, ia, ib);
-                        const int a = sa + ia, b = sB + ib;
-                        const float4 ua = v.u[a], ub = v.u[b];
-                        const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
-                        int dcur = -1;
-                        float damp = 0.f;
-#pragma unroll
-                        for (int f = 0; f < SYMM_CHUNK; ++f) {
-                            if (f < nf) {
-                                const float4 q = v.par[f0 + f];
-                                const int pk = __float_as_int(q.w);
-                                const int d = pk & 0xff, iz = (pk >> 8) - 1;
-                                if (d != dcur) {
-                                    dcur = d;
-                                    damp = v.w[d * cap + a] * v.w[d * cap + b];
-                                }
-                                float pz, pm1;
-                                ang_pow(cs, q.x, q.y, iz, pz, pm1);
-                                acc[f] = fmaf(pz, damp, acc[f]);
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int f = 0; f < SYMM_CHUNK; ++f) {
-                        if (f < nf) {
-                            const float s = warp_sum(acc[f]);
-                            if (lane == 0) Gi[B.off_g + f0 + f] = s;
-                        }
-                    }
-                }
-            } else {
-                // other forms: one function per pass over the pairs
-                for (int f = 0; f < B.n; ++f) {
-                    const float4 q = v.par[f];
-                    const int iz = (__float_as_int(q.w) >> 8) - 1;
-                    float acc = 0.f;
-                    for (int p = lane; p < npairs; p += 32) {
-                        int ia, ib;
-                        pair_at(tri, nb, p, ia, ib);
-                        const int a = sa + ia, b = sB + ib;
-                        const float4 ua = v.u[a], ub = v.u[b];
-                        const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
-                        float h, hc, hrj, hrk;
-                        angular_generic(B.form, ua.w, ub.w, cs, v.fc[B.cut * cap + a], v.fc[B.cut * cap + b], 0.f,
-                                        0.f, q.x, q.y, iz, q.z, false, h, hc, hrj, hrk);
-                        acc += h;
-                    }
-                    acc = warp_sum(acc);
-                    if (lane == 0) Gi[B.off_g + f] = acc;
-                }
-            }
-            __syncwarp();
-        }
-        __syncwarp();
-    }
+    symm_body<Acc, GenericBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, G,
+                                  reinterpret_cast<float *>(smem4));
 }
 
 // ------------------------------------------------------------------ networks (FP32)
@@ -746,200 +504,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_nn_fp32(int64_t N, const DevPot 
 
 // ------------------------------------------------------------------ forces
 
-// One warp per atom.  With e = dE_i/dG_i, every pair and triplet contributes
-// dE_i/dd_j for the neighbour displacements d_j = x_i - x_j - R q.  For a
-// triplet (a,b) with dE/dcos = hc, dE/dr_a = hra, dE/dr_b = hrb:
-//   dE/dd_a = (hra - hc cos/r_a) u_a + (hc/r_a) u_b,  and a <-> b.
-// The warp writes these four coefficients per pair of a block into shared
-// memory, then every lane owns neighbour slots and sums their pairs in a
-// fixed order (no atomics).  Finally F_j += g_j and F_i -= sum_j g_j in FP64
-// -- the Newton-3 scatter of nnp.cpp:443-471.
 __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot *__restrict__ pot,
                                                         const float2 *__restrict__ rpar, const float4 *__restrict__ apar,
-                                                        const int *__restrict__ type, const float4 *__restrict__ nbr,
+                                                        const int *__restrict__ type, const int *__restrict__ order, const float4 *__restrict__ nbr,
                                                         const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
                                                         int gstride, const float *__restrict__ dEdG,
                                                         double *__restrict__ F, DevErr *err)
 {
     extern __shared__ float4 smem4[];
-    float *smem = reinterpret_cast<float *>(smem4);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
-    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
-    float *cA = v.pc, *cB = v.pc + PCH, *cC = v.pc + 2 * PCH, *cD = v.pc + 3 * PCH;
-    const DevPot &P = *pot;
-    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
-        const int II = type[i];
-        const DevType &T = P.t[II];
-        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
-        const float *e = dEdG + i * gstride;
-        for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
-        __syncwarp();
-        // ---- radial: lanes own their neighbour slot (initialises g)
-        for (int k = lane; k < n; k += 32) {
-            const DevBlockR B = T.br[v.t[k]];
-            const float4 u = v.u[k];
-            const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
-            float amp = 0.f;
-            for (int f = 0; f < B.n; ++f) {
-                const float2 q = rpar[B.par + f];
-                float val, der;
-                radial_fd(B.form, u.w, q.x, q.y, fc, fd, val, der);
-                amp = fmaf(v.vec[B.off_g + f], der, amp);
-            }
-            v.gx[k] = amp * u.x;
-            v.gy[k] = amp * u.y;
-            v.gz[k] = amp * u.z;
-        }
-        __syncwarp();
-        // ---- angular
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
-            const DevBlockA B = T.ba[tt];
-            if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
-            const int sa = v.seg[J], na = v.seg[J + 1] - sa;
-            const int sb0 = v.seg[K], nb = v.seg[K + 1] - sb0;
-            const bool tri = (J == K);
-            const int sb = tri ? sa : sb0;
-            const int npairs = tri ? na * (na - 1) / 2 : na * nb;
-            if (npairs == 0) continue;
-            for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
-            __syncwarp();
-            const float *eb = v.vec + B.off_g;
-            const bool gauss = (B.form == ANG_GAUSS);
-            for (int c0 = 0; c0 < npairs; c0 += PCH) {
-                const int c1 = min(npairs, c0 + PCH);
-                // -- pair pass: coefficients of the two per-slot gradients
-                for (int p = c0 + lane; p < c1; p += 32) {
-                    int ia, ib;
-                    pair_at(tri, nb, p, ia, ib);
-                    const int a = sa + ia, b = sb + ib;
-                    const float4 ua = v.u[a], ub = v.u[b];
-                    const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
-                    float hc = 0.f, hra = 0.f, hrb = 0.f;   // dE/dcos, dE/dr_a, dE/dr_b
-                    if (gauss) {
-                        int dcur = -1;
-                        float sc = 0.f, sp = 0.f;
-                        for (int f = 0; f < B.n; ++f) {
-                            const float4 q = v.par[f];
-                            const int pk = __float_as_int(q.w);
-                            const int d = pk & 0xff, iz = (pk >> 8) - 1;
-                            if (d != dcur) {
-                                if (dcur >= 0) {
-                                    const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
-                                    hc = fmaf(sc, wa * wb, hc);
-                                    hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
-                                    hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
-                                }
-                                dcur = d;
-                                sc = 0.f;
-                                sp = 0.f;
-                            }
-                            float pz, pm1;
-                            ang_pow(cs, q.x, q.y, iz, pz, pm1);
-                            const float ef = eb[f];
-                            sc = fmaf(ef * q.y * q.x, pm1, sc);
-                            sp = fmaf(ef, pz, sp);
-                        }
-                        if (dcur >= 0) {
-                            const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
-                            hc = fmaf(sc, wa * wb, hc);
-                            hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
-                            hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
-                        }
-                    } else {
-                        const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];
-                        const float ga = v.fd[B.cut * cap + a], gb = v.fd[B.cut * cap + b];
-                        for (int f = 0; f < B.n; ++f) {
-                            const float4 q = v.par[f];
-                            const int iz = (__float_as_int(q.w) >> 8) - 1;
-                            float h, dc, dra, drb;
-                            angular_generic(B.form, ua.w, ub.w, cs, ca, cb, ga, gb, q.x, q.y, iz, q.z, true, h, dc, dra,
-                                            drb);
-                            const float ef = eb[f];
-                            hc = fmaf(ef, dc, hc);
-                            hra = fmaf(ef, dra, hra);
-                            hrb = fmaf(ef, drb, hrb);
-                        }
-                    }
-                    const float ira = 1.f / ua.w, irb = 1.f / ub.w;
-                    cA[p - c0] = hra - hc * cs * ira;   // on u_a in dE/dd_a
-                    cB[p - c0] = hc * ira;              // on u_b in dE/dd_a
-                    cC[p - c0] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
-                    cD[p - c0] = hc * irb;              // on u_a in dE/dd_b
-                }
-                __syncwarp();
-                // -- slot pass: each lane sums the pairs of the slots it owns
-                const int nslots = tri ? na : na + nb;
-                for (int sl = lane; sl < nslots; sl += 32) {
-                    const bool is_row = tri || sl < na;       // first member of its pairs
-                    const bool is_col = tri || sl >= na;      // second member
-                    const int ir = tri ? sl : sl;             // row index if is_row
-                    const int ic = tri ? sl : sl - na;        // column index if is_col
-                    const int slot = (tri || sl < na) ? sa + sl : sb + ic;
-                    const float4 us = v.u[slot];
-                    float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-                    if (is_row) {
-                        const int rs = tri ? ir * (ir - 1) / 2 : ir * nb;
-                        const int rl = tri ? ir : nb;
-                        const int p0 = max(rs, c0), p1 = min(rs + rl, c1);
-                        for (int p = p0; p < p1; ++p) {
-                            const float4 ub = v.u[sb + (p - rs)];
-                            sa_ += cA[p - c0];
-                            const float bt = cB[p - c0];
-                            vx = fmaf(bt, ub.x, vx);
-                            vy = fmaf(bt, ub.y, vy);
-                            vz = fmaf(bt, ub.z, vz);
-                        }
-                    }
-                    if (is_col) {
-                        for (int ra = tri ? ic + 1 : 0; ra < na; ++ra) {
-                            const int p = (tri ? ra * (ra - 1) / 2 : ra * nb) + ic;
-                            if (p < c0) continue;
-                            if (p >= c1) break;
-                            const float4 ua = v.u[sa + ra];
-                            sa_ += cC[p - c0];
-                            const float dt = cD[p - c0];
-                            vx = fmaf(dt, ua.x, vx);
-                            vy = fmaf(dt, ua.y, vy);
-                            vz = fmaf(dt, ua.z, vz);
-                        }
-                    }
-                    v.gx[slot] += fmaf(sa_, us.x, vx);
-                    v.gy[slot] += fmaf(sa_, us.y, vy);
-                    v.gz[slot] += fmaf(sa_, us.z, vz);
-                }
-                __syncwarp();
-            }
-        }
-        __syncwarp();
-        // ---- scatter: F_j += g_j, F_i -= sum g_j
-        double fx = 0.0, fy = 0.0, fz = 0.0;
-        bool bad = false;
-        for (int k = lane; k < n; k += 32) {
-            const float gx = v.gx[k], gy = v.gy[k], gz = v.gz[k];
-            bad |= !(isfinite(gx) && isfinite(gy) && isfinite(gz));
-            const int64_t j = v.j[k];
-            atomicAdd(&F[3 * j], (double)gx);
-            atomicAdd(&F[3 * j + 1], (double)gy);
-            atomicAdd(&F[3 * j + 2], (double)gz);
-            fx += gx;
-            fy += gy;
-            fz += gz;
-        }
-        fx = warp_sum_d(fx);
-        fy = warp_sum_d(fy);
-        fz = warp_sum_d(fz);
-        if (lane == 0) {
-            atomicAdd(&F[3 * i], -fx);
-            atomicAdd(&F[3 * i + 1], -fy);
-            atomicAdd(&F[3 * i + 2], -fz);
-        }
-        if (__any_sync(FULL, bad) && lane == 0) atomicMax(&err->nonfinite, 1);
-        __syncwarp();
-    }
+    force_body<GenericBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, dEdG, F, err,
+                              reinterpret_cast<float *>(smem4));
 }
 
 // ------------------------------------------------------------------ energies
@@ -1049,6 +623,8 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.cell_fill.reserve(cell_bound));
     r(E.cell_atoms.reserve(N));
     r(E.cell_pos.reserve(N));
+    r(E.order.reserve(N));
+    r(E.type_fill.reserve(2 * NNP_MAX_TYPES));
     r(E.nbr.reserve(N * (size_t)E.cap));
     r(E.nbr_cnt.reserve(N));
     r(E.G.reserve(N * (size_t)E.gstride));
@@ -1069,7 +645,11 @@ std::string run_neighbors(Engine &E, int pbc)
     if (N == 0 || S == 0) return "";
     cudaStream_t st = E.stream;
     E.mark(0);
-    E.launches += 10;
+    E.launches += 12;
+    cudaMemsetAsync(E.type_fill.p, 0, 2 * NNP_MAX_TYPES * sizeof(int), st);
+    k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p);
+    k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p,
+                                                               E.type_fill.p + NNP_MAX_TYPES, E.order.p);
     k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
                                                              E.dpot.ntypes, E.err.p);
     k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
@@ -1096,11 +676,21 @@ std::string run_symm(Engine &E)
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
     const size_t sm = view_bytes(E, false);
-    cudaFuncSetAttribute(k_symm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_symm<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
-        N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
-        E.G.p);
+    const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
+    if (E.use_jit && E.jit_symm && !E.acc64) {
+        long long n = N;
+        int cap = E.cap, nc = ncut_max(E), nd = ndamp_max(E), gs = E.gstride;
+        void *args[] = {&n, &E.d_pot, &E.rpar.p, &E.apar.p, &E.type.p, &E.order.p, &E.nbr.p, &E.nbr_cnt.p,
+                        &cap, &nc, &nd, &gs, &E.G.p};
+        std::string msg = jit_launch(E.jit_symm, grid, WARPS * 32, sm, E.stream, args);
+        E.mark(2);
+        return msg;
+    }
+    auto kern = E.acc64 ? k_symm<double> : k_symm<float>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<grid, WARPS * 32, sm, E.stream>>>(N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.order.p, E.nbr.p, E.nbr_cnt.p, E.cap,
+                                             ncut_max(E), ndamp_max(E), E.gstride, E.G.p);
     E.mark(2);
     return cuda_msg("symmetry functions");
 }
@@ -1134,11 +724,20 @@ std::string run_force(Engine &E)
     if (N == 0) return "";
     cudaMemsetAsync(E.force.p, 0, 3 * (size_t)N * sizeof(double), E.stream);
     const size_t sm = view_bytes(E, true);
-    cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_force<<<grid_for(N, WARPS, num_sms() * 16), WARPS * 32, sm, E.stream>>>(
-        N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut_max(E), ndamp_max(E), E.gstride,
-        E.dEdG.p, E.force.p, E.err.p);
+    const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
+    if (E.use_jit && E.jit_force) {
+        long long n = N;
+        int cap = E.cap, nc = ncut_max(E), nd = ndamp_max(E), gs = E.gstride;
+        void *args[] = {&n, &E.d_pot, &E.rpar.p, &E.apar.p, &E.type.p, &E.order.p, &E.nbr.p, &E.nbr_cnt.p,
+                        &cap, &nc, &nd, &gs, &E.dEdG.p, &E.force.p, &E.err.p};
+        std::string msg = jit_launch(E.jit_force, grid, WARPS * 32, sm, E.stream, args);
+        E.mark(4);
+        return msg;
+    }
+    cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_force<<<grid, WARPS * 32, sm, E.stream>>>(N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.order.p, E.nbr.p, E.nbr_cnt.p, E.cap,
+                                                ncut_max(E), ndamp_max(E), E.gstride, E.dEdG.p, E.force.p, E.err.p);
     E.mark(4);
     return cuda_msg("forces");
 }

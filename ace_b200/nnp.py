@@ -64,6 +64,9 @@ def lib():
             "nnp_get_params": ([p, p], i),
             "nnp_set_params": ([p, p], i),
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
+            "nnp_set_accumulation": ([p, i], i),
+            "nnp_set_specialization": ([p, i], i),
+            "nnp_specialization": ([p, C.POINTER(i), C.POINTER(C.c_char_p)], i),
             "nnp_set_timing": ([p, i], i),
             "nnp_stage_times": ([p, p, i], i),
             "nnp_neighbor_counts": ([p, p], i),
@@ -162,6 +165,21 @@ class NNP:
 
     def set_precision(self, prec: int):
         self._check(lib().nnp_set_precision(self._h, prec))
+
+    def set_accumulation(self, fp64: bool = True):
+        """FP64 (default) or FP32 running sums of the symmetry functions."""
+        self._check(lib().nnp_set_accumulation(self._h, 1 if fp64 else 0))
+
+    def set_specialization(self, on: bool = True):
+        """Use the kernels compiled for this basis at creation (True) or the prebuilt ones."""
+        self._check(lib().nnp_set_specialization(self._h, 1 if on else 0))
+
+    def specialization(self):
+        """(active, CUDA source of the specialised kernels)."""
+        a = C.c_int32()
+        s = C.c_char_p()
+        self._check(lib().nnp_specialization(self._h, C.byref(a), C.byref(s)))
+        return bool(a.value), (s.value or b"").decode()
 
     def set_stream(self, stream_ptr: int):
         self._check(lib().nnp_set_stream(self._h, C.c_void_p(stream_ptr)))

@@ -11,9 +11,9 @@ name.  Choices the configurations leave open are fixed as follows:
   (the reference's eta is a length: exp(-(rij^2+rik^2)/eta^2)), eta
   outermost so equal-eta runs share one damping factor, then
   zeta in {1,2,4,8} and lambda = +-1;
-* an angular block of m functions takes ceil(m/2) functions of the first
-  eta and the rest of the second, each run walking
-  (1,+1),(1,-1),(2,+1),(2,-1),... in (zeta, lambda);
+* an angular block of m functions takes m evenly spaced members of the
+  16-function set eta x zeta x lambda (eta outermost), so every block
+  spans zeta up to 8;
 * networks are tanh with a linear output, Xavier-normal weights
   (sigma_w = 1), biases N(0, 0.001 * Xavier scale) (ml/nn.cpp:1193-1209);
 * batched structures place atoms on a randomly chosen subset of a jittered
@@ -71,16 +71,13 @@ class Batch:
 
 
 def angular_params(m: int):
-    pat = [(z, l) for z in (1.0, 2.0, 4.0, 8.0) for l in (1, -1)]
-    n1 = (m + 1) // 2
-    eta, zeta, lam = [], [], []
-    for k in range(m):
-        e = ETA_A[0] if k < n1 else ETA_A[1]
-        z, l = pat[k if k < n1 else k - n1]
-        eta.append(e)
-        zeta.append(z)
-        lam.append(l)
-    return np.array(eta), np.array(zeta), np.array(lam, dtype=np.int32)
+    """m functions picked evenly from the 16-function set ordered eta-outermost:
+    eta in ETA_A x (zeta, lambda) in (1,+1),(1,-1),(2,+1),(2,-1),...,(8,-1)."""
+    full = [(e, z, l) for e in ETA_A for z in (1.0, 2.0, 4.0, 8.0) for l in (1, -1)]
+    idx = np.round(np.linspace(0, len(full) - 1, m)).astype(int) if m > 1 else np.array([0])
+    pick = [full[k] for k in idx]
+    return (np.array([p[0] for p in pick]), np.array([p[1] for p in pick]),
+            np.array([p[2] for p in pick], dtype=np.int32))
 
 
 def xavier_net(rng: np.random.Generator, nodes: Sequence[int], neuron: str = "TANH") -> Network:

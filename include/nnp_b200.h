@@ -92,6 +92,27 @@ int nnp_write(const nnp_handle *h, const char *path);
 /* Network-layer precision (NNP_PREC_*). */
 int nnp_set_precision(nnp_handle *h, int32_t precision);
 
+/* Running sums of the symmetry functions: NNP_ACC_FP64 adds every
+ * FP32 pair/triplet term into an FP64 sum; NNP_ACC_FP32 (default) keeps FP32 sums
+ * (faster; ~sqrt(T/32) ulp error for T triplets per atom). */
+#define NNP_ACC_FP32 0
+#define NNP_ACC_FP64 1
+int nnp_set_accumulation(nnp_handle *h, int32_t acc);
+
+/* Kernels specialised for the loaded basis.  At creation the library writes
+ * CUDA source in which every GAUSS angular block is straight-line code with its
+ * parameters as literals and compiles it for sm_100a with NVRTC (environment
+ * NNP_JIT=0 skips this).  enable=0 switches back to the prebuilt kernels;
+ * nnp_specialization reports whether the specialised kernels are in use and
+ * returns their source text. */
+int nnp_set_specialization(nnp_handle *h, int32_t enable);
+int nnp_specialization(const nnp_handle *h, int32_t *active, const char **source);
+
+/* Writes and compiles the specialised kernels of a potential file without a GPU
+ * (NVRTC only); log receives the generated source, or the compiler's message
+ * when compilation fails (NNP_ERR_CUDA). */
+int nnp_specialization_check(const char *potential_path, char *log, int32_t log_len);
+
 /* Launch on this CUDA stream (cudaStream_t) instead of the handle's own one. */
 int nnp_set_stream(nnp_handle *h, void *cuda_stream);
 
