@@ -45,7 +45,7 @@ WORKLOAD = "batched inference: 4096 structures x U{16..512} atoms, 3 elements, 5
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--structures", type=int, default=4096)
@@ -199,6 +199,16 @@ def cpu_reference(path: str, batch, n_sample: int, procs: int):
     return atoms / dt, dt, atoms, ordered
 
 
+# DRAM bytes per atom of one launch, from the ncu capture of the 512-structure
+# case of this workload (dram__bytes_read.sum + dram__bytes_write.sum / atoms)
+DRAM_BYTES_PER_ATOM = {"k_force_jit": 145.647616e6 / 134400, "k_symm_jit": 118.50496e6 / 134400}
+
+
+def traffic_bytes(kernel: str, atoms: int):
+    b = DRAM_BYTES_PER_ATOM.get(kernel)
+    return None if b is None else round(b * atoms)
+
+
 def ref_kind():
     return "port"
 
@@ -324,12 +334,17 @@ def main():
     n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_fp32 = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
     achieved = flo / (per_step[kern] / 1e3) / 1e12
-    roofline = {"bound": "fp32", "kernel": "k_" + ("symm" if kern == "symm" else "force"),
+    jit = bool(nn.specialization()[0])
+    kname = ("k_symm" if kern == "symm" else "k_force") + ("_jit" if jit else "")
+    roofline = {"bound": "fp32", "kernel": kname,
                 "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4),
                 "peak_source": "%d SMs x 128 FP32 FMA/clk x 2 x measured %.0f MHz (no FP32 figure in MEASURED_PEAKS.json)"
                                % (n_sm, sm_mhz),
-                "traffic": None}
+                "traffic": traffic_bytes(kname, N)}
+    if roofline["traffic"] is not None:
+        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one %s launch on the "
+                                      "first 512 structures (134,400 atoms), scaled by atoms" % kname)
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
