@@ -712,6 +712,35 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
     return rc;
 }
 
+int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, const int64_t *d_atom_off,
+                            const int32_t *d_type, const float *d_symm, int32_t gstride, uint32_t flags,
+                            double *d_energy)
+{
+    if (!h) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (n_struct < 0 || n_atoms < 0) return fail(h, NNP_ERR_ARG, "negative structure or atom count");
+    if (flags & ~(uint32_t)NNP_VACUUM) return fail(h, NNP_ERR_ARG, "flags other than NNP_VACUUM");
+    if (n_atoms > NNP_NOALLOC_MAX_ATOMS)
+        return fail(h, NNP_ERR_CAPACITY, "allocation-free call takes at most " + std::to_string(NNP_NOALLOC_MAX_ATOMS) +
+                                             " atoms, got " + std::to_string(n_atoms));
+    if (E.precision != NNP_PREC_FP32) return fail(h, NNP_ERR_UNSUPPORTED, "this build implements the FP32 network path only");
+    int nin = 0;
+    for (int t = 0; t < E.dpot.ntypes; ++t) nin = std::max(nin, E.dpot.t[t].n_input);
+    if (gstride < nin) return fail(h, NNP_ERR_ARG, "gstride " + std::to_string(gstride) + " is below the largest input size " + std::to_string(nin));
+    if (n_struct == 0) return NNP_OK;
+    if (!d_atom_off || !d_energy || (n_atoms > 0 && (!d_type || !d_symm))) return fail(h, NNP_ERR_ARG, "null device pointer");
+    // the handle's tables live on the device it was created on; that device must be current
+    cudaPointerAttributes pa;
+    int dev = -1;
+    if (cudaPointerGetAttributes(&pa, E.d_pot) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess || pa.device != dev) {
+        cudaGetLastError();
+        return fail(h, NNP_ERR_ARG, "the handle's device is not the current device");
+    }
+    std::string msg = nnp::run_energy_symm_noalloc(E, n_struct, n_atoms, d_atom_off, d_type, d_symm, gstride,
+                                                   (flags & NNP_VACUUM) != 0, d_energy);
+    return msg.empty() ? NNP_OK : fail(h, NNP_ERR_CUDA, msg);
+}
+
 int nnp_compute_energy_symm(nnp_handle *h, int32_t n_struct, const int64_t *atom_off, const int32_t *type,
                             const double *symm, int32_t gstride, double *energy)
 {

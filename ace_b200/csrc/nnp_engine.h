@@ -124,6 +124,8 @@ std::string run_energy(Engine &E, bool vacuum);
 std::string run_symm_to_double(Engine &E, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
+std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,
+                                    const float *G, int gstride, bool vacuum, double *energy);
 
 // run-time specialised kernels (nnp_jit.cpp)
 std::string jit_compile(const Engine &E, std::string &source, std::vector<char> &cubin);

@@ -19,7 +19,9 @@
 //                  (NNP::compute_force, nnp/nnp.cpp:412-476)
 //   k_energy       one block per structure, FP64 energy sum
 #include <cstdio>
+#include <mutex>
 
+#include "../../include/nnp_b200.h"
 #include "nnp_device.cuh"
 #include "nnp_engine.h"
 
@@ -767,6 +769,145 @@ std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in)
     if (n == 0) return "";
     k_d2f<<<grid_for(n, 256, 1 << 30), 256, 0, E.stream>>>(n, symm_d, E.G.p);
     return run_nn(E);
+}
+
+// ------------------------------------------------------------------ allocation-free energies
+//
+// Energies of a batch from device-resident symmetry functions for callers
+// that must not allocate device memory during the call (a serving loop that
+// has reserved all of its memory up front, or one running under an external
+// allocator): cudaMalloc/cudaFree synchronise the whole device and can fail
+// under memory pressure.  The only scratch, one FP32 energy per atom, lives
+// in this file-scope array, so the call's size limit is NNP_NOALLOC_MAX_ATOMS
+// atoms.  Every call writes entries [0, N) before it reads them (same
+// stream, kernel order), so the array needs no initial contents.  It is one
+// array per device, shared by every handle on that device: calls that may
+// overlap in time (different streams or host threads) race on it and must be
+// ordered by the caller.
+
+static __device__ __align__(256) float g_noalloc_e_atom[NNP_NOALLOC_MAX_ATOMS];
+
+// Forward pass only (the energy half of k_nn_fp32, same arithmetic order);
+// an atom whose type is outside [0, ntypes) gets a NaN energy.
+__global__ void __launch_bounds__(WARPS * 32) k_nn_energy_fp32(int64_t N, const DevPot *__restrict__ pot,
+                                                              const float *__restrict__ wpar, int64_t wfloats,
+                                                              const int *__restrict__ type,
+                                                              const float *__restrict__ G, int gstride, int maxn,
+                                                              float *__restrict__ e_atom)
+{
+    extern __shared__ float smem[];
+    float *w_s = smem;
+    for (int64_t k = threadIdx.x; k < wfloats; k += blockDim.x) w_s[k] = wpar[k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *xa = smem + ((wfloats + 3) & ~3) + (size_t)warp * 2 * maxn;
+    float *xb = xa + maxn;
+    const DevPot &P = *pot;
+    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
+        const int ti = type[i];
+        if (ti < 0 || ti >= P.ntypes) {
+            if (lane == 0) e_atom[i] = __int_as_float(0x7fffffff);
+            continue;
+        }
+        const DevType &T = P.t[ti];
+        const NetView V = net_view(w_s + T.woff, T);
+        const int L = T.nlayer, nin = T.nodes[0];
+        const float *Gi = G + i * gstride;
+        for (int m = lane; m < nin; m += 32) xa[m] = V.inpw[m] * (Gi[m] + V.inpb[m]);
+        __syncwarp();
+        float *x = xa, *y = xb;
+        for (int l = 0; l < L; ++l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], s = V.ws[l];
+            const int neu = (l == L - 1) ? NEU_LINEAR : T.neuron;
+            for (int n = lane; n < no; n += 32) {
+                float z = V.b[l][n];
+                const float *wc = V.wt[l] + n;
+                for (int m = 0; m < ni; ++m) z += wc[m * s] * x[m];
+                float a, d, d2;
+                activation(neu, T.c, z, a, d, d2);
+                y[n] = a;
+            }
+            __syncwarp();
+            float *tmp = x; x = y; y = tmp;
+        }
+        if (lane == 0) e_atom[i] = V.outb[0] + x[0] * V.outw[0];
+        __syncwarp();
+    }
+}
+
+// One block per structure, FP64 sum (as k_energy); an out-of-range type
+// with vacuum energies requested gives NaN, and so does a structure whose
+// offsets fall outside [0, N] (nothing outside the N scratch entries is read).
+__global__ void k_energy_noalloc(const int64_t *__restrict__ off, int64_t N, const float *__restrict__ e_atom,
+                                 const int *__restrict__ type, int ntypes, int vacuum,
+                                 const double *__restrict__ vac, double *__restrict__ e_struct)
+{
+    __shared__ double part[256];
+    const int s = blockIdx.x;
+    const int64_t a0 = off[s], a1 = off[s + 1];
+    if (a0 < 0 || a1 < a0 || a1 > N) {
+        if (threadIdx.x == 0) e_struct[s] = __longlong_as_double(0x7ff8000000000000ll);
+        return;
+    }
+    double sum = 0.0;
+    for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        sum += (double)e_atom[a];
+        if (vacuum) {
+            const int t = type[a];
+            sum += (t >= 0 && t < ntypes) ? vac[t] : __longlong_as_double(0x7ff8000000000000ll);
+        }
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int d = blockDim.x / 2; d; d >>= 1) {
+        if (threadIdx.x < d) part[threadIdx.x] += part[threadIdx.x + d];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) e_struct[s] = part[0];
+}
+
+// Device address of the scratch array on the current device, looked up once
+// per device (cudaGetSymbolAddress may load the module; it allocates nothing
+// the caller owns).
+std::string noalloc_scratch(float **out)
+{
+    static std::mutex mu;
+    static float *addr[256] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    if (dev < 0 || dev >= 256) return "device ordinal out of range";
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        float *p = nullptr;
+        e = cudaGetSymbolAddress((void **)&p, g_noalloc_e_atom);
+        if (e != cudaSuccess) return std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return "";
+}
+
+std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,
+                                    const float *G, int gstride, bool vacuum, double *energy)
+{
+    float *e_atom = nullptr;
+    std::string msg = noalloc_scratch(&e_atom);
+    if (!msg.empty()) return msg;
+    if (S == 0) return "";
+    const int maxn = max_nodes(E);
+    const size_t sm = (size_t)(((E.wfloats + 3) & ~3) + WARPS * 2 * maxn) * sizeof(float);
+    if (sm > 220 * 1024) return "networks too large for the shared-memory FP32 path";
+    if (N > 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_nn_energy_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+        k_nn_energy_fp32<<<grid_for(N, WARPS * 8, num_sms() * 2), WARPS * 32, sm, E.stream>>>(
+            N, E.d_pot, E.wpar.p, E.wfloats, type, G, gstride, maxn, e_atom);
+        E.launches += 1;
+    }
+    k_energy_noalloc<<<S, 256, 0, E.stream>>>(off, N, e_atom, type, E.dpot.ntypes, vacuum ? 1 : 0, E.vac.p, energy);
+    E.launches += 1;
+    return cuda_msg("allocation-free energies");
 }
 
 }  // namespace nnp

@@ -166,6 +166,31 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);
 
+/* Allocation-free energies from device-resident symmetry functions (no
+ * counterpart in the reference, whose NNP::compute_energy (nnp.cpp:329-338)
+ * it otherwise follows).  For callers that must not allocate device memory
+ * during the call -- cudaMalloc/cudaFree synchronise the device and can fail
+ * once a serving process has reserved its memory -- this call allocates
+ * nothing: its only scratch (one float per atom) is a fixed array inside the
+ * library, so a call takes at most NNP_NOALLOC_MAX_ATOMS atoms (larger
+ * batches return NNP_ERR_CAPACITY before anything is launched).
+ *  d_atom_off[n_struct+1], d_type[n_atoms], d_symm[n_atoms*gstride] (FP32 rows,
+ *  gstride >= the largest nnp_n_input), d_energy[n_struct] (FP64 out) are
+ *  device pointers on the handle's device, which must be current; n_atoms
+ *  must equal d_atom_off[n_struct] (a structure whose offsets fall outside
+ *  [0, n_atoms] gets a NaN energy).  flags: 0 or NNP_VACUUM.
+ * The kernels are queued on the handle's stream and the call returns without
+ * waiting for them.  An atom type outside [0, ntypes) gives a NaN energy for
+ * its structure.  The first call on a device looks up the scratch array's
+ * address, which may load the library's device code; make that first call
+ * before any stream capture.  The scratch array is one per device, shared by
+ * all handles: calls that can overlap in time (other streams, other host
+ * threads) race on it and must be ordered by the caller. */
+#define NNP_NOALLOC_MAX_ATOMS (1 << 20)
+int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, const int64_t *d_atom_off,
+                            const int32_t *d_type, const float *d_symm, int32_t gstride, uint32_t flags,
+                            double *d_energy);
+
 /* Stage timers, the device-side counterpart of the reference's phase clocks
  * ("time - symm/energy/force", nnptefr.cpp:2863-2885, 3547-3592).  When enabled,
  * nnp_compute records CUDA events between its stages; nnp_stage_times then
