@@ -17,7 +17,7 @@ symmetry functions, networks, forces, per-structure energies.
           energies and forces inside the timed region (wall clock).
 
 --impl reference times the reference's CPU implementation of the path on
-this host's cores (the compiled reference when oracle/_ref holds it, else
+this host's cores (the reference's own code compiled in oracle/_ref, else
 the FP64 restatement in oracle/), on a bounded sample of the same workload.
 """
 from __future__ import annotations
@@ -167,11 +167,21 @@ class ClockSampler:
 # ---------------------------------------------------------------- CPU reference
 
 def _ref_worker(args):
-    path, chunk = args
+    """NeighborList::build + compute_symm + compute_force per structure: the
+    reference's own code (oracle/_ref) when built, else the FP64 port."""
+    path, chunk, kind = args
     sys.path.insert(0, ROOT)
+    out = []
+    if kind == "reference":
+        from oracle import ref
+        rp = ref.RefNNP(path)
+        for (p, t, c) in chunk:
+            e, f, _, _ = rp.compute(p, t, c)
+            out.append((e, f))
+        rp.close()
+        return out
     from oracle import oracle as orc
     op = orc.OraclePot.from_file(path)
-    out = []
     for (p, t, c) in chunk:
         e, f, _ = orc.compute(op, p, t, c)
         out.append((e, f))
@@ -187,9 +197,10 @@ def cpu_reference(path: str, batch, n_sample: int, procs: int):
     chunks = [structs[k::procs] for k in range(procs)]
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        pool.map(_ref_worker, [(path, [structs[0]])] * procs)       # import / warm-up
+        kind = ref_kind()
+        pool.map(_ref_worker, [(path, [structs[0]], kind)] * procs)       # import / warm-up
         t0 = time.perf_counter()
-        res = pool.map(_ref_worker, [(path, ch) for ch in chunks])
+        res = pool.map(_ref_worker, [(path, ch, kind) for ch in chunks])
         dt = time.perf_counter() - t0
     ordered = [None] * len(structs)
     for k in range(procs):
@@ -210,7 +221,9 @@ def traffic_bytes(kernel: str, atoms: int):
 
 
 def ref_kind():
-    return "port"
+    """"reference" when the reference's own code is built in oracle/_ref."""
+    from oracle import ref
+    return "reference" if ref.available() else "port"
 
 
 # ---------------------------------------------------------------- main

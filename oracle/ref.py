@@ -1,0 +1,87 @@
+"""ctypes wrapper of the reference's own NNP code compiled into
+oracle/_ref/libref.so by oracle/ref/Makefile (from the reference sources,
+with the project's small Eigen header).
+
+TEST INFRASTRUCTURE ONLY: used by the tests (to pin the oracle and the CUDA
+path to the reference), by tests/golden/make_golden.py, and by bench.py's
+CPU baseline / reference arm.  Never used by the library."""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "_ref", "libref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIBPATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise ImportError("oracle/_ref/libref.so is not built (make -C oracle/ref)")
+        L = C.CDLL(LIBPATH)
+        p = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.ref_nnp_read.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.ref_nnp_read.restype = p
+        L.ref_nnp_free.argtypes = [p]
+        L.ref_nnp_ntypes.argtypes = [p]
+        L.ref_nnp_rc.argtypes = [p]
+        L.ref_nnp_rc.restype = C.c_double
+        L.ref_nnp_ninput.argtypes = [p, C.c_int]
+        L.ref_nnp_compute.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, C.c_int, dp, dp, dp, dp,
+                                      C.c_char_p, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class RefNNP:
+    """The reference's NNP read from a potential file."""
+
+    def __init__(self, path: str):
+        err = C.create_string_buffer(512)
+        self.h = lib().ref_nnp_read(os.fsencode(path), err, len(err))
+        if not self.h:
+            raise RuntimeError("reference NNP::read failed: " + err.value.decode())
+        self.ntypes = lib().ref_nnp_ntypes(self.h)
+        self.rc = lib().ref_nnp_rc(self.h)
+        self.gstride = max(lib().ref_nnp_ninput(self.h, t) for t in range(self.ntypes))
+
+    def close(self):
+        if self.h:
+            lib().ref_nnp_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compute(self, pos, types, cell, pbc=True, want_symm=False):
+        """One structure through NNP::compute_symm + compute_force (+
+        compute_energy): returns (energy without vacuum terms, forces [n,3],
+        energy with vacuum terms, symm [n, gstride] or None)."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        cell = np.ascontiguousarray(cell if cell is not None else np.zeros(9), dtype=np.float64).reshape(9)
+        e = np.zeros(1)
+        ev = np.zeros(1)
+        f = np.zeros((max(n, 1), 3))
+        g = np.zeros((max(n, 1), self.gstride)) if want_symm else None
+        err = C.create_string_buffer(512)
+        rc = lib().ref_nnp_compute(self.h, n, _dp(pos), types.ctypes.data_as(C.POINTER(C.c_int)), _dp(cell),
+                                   1 if pbc else 0, self.gstride, _dp(e), _dp(f), _dp(g), _dp(ev), err, len(err))
+        if rc != 0:
+            raise RuntimeError("reference compute failed: " + err.value.decode())
+        return float(e[0]), f[:n], float(ev[0]), (g[:n] if want_symm else None)
