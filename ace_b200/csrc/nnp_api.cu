@@ -68,6 +68,7 @@ void Engine::free_all()
     cell_pos.release(); order.release(); type_fill.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release();
+    tvec.release(); gE.release(); tang.release(); pgrad.release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
     d_pot = nullptr;
@@ -832,10 +833,100 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
 int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, const double *f_ref, double w_f,
                    int32_t norm_mode, double *loss, double *grad, double *e_out, double *f_out, uint32_t flags)
 {
-    (void)batch; (void)e_ref; (void)f_ref; (void)w_f; (void)norm_mode; (void)loss; (void)grad; (void)e_out;
-    (void)f_out; (void)flags;
-    if (!h) return NNP_ERR_ARG;
-    return fail(h, NNP_ERR_UNSUPPORTED, "nnp_train_grad is not built yet");
+    if (!h || !batch) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (flags & NNP_DEVICE_PTRS) return fail(h, NNP_ERR_UNSUPPORTED, "nnp_train_grad takes host pointers");
+    if (!e_ref || !loss || !grad) return fail(h, NNP_ERR_ARG, "e_ref, loss and grad are required");
+    if (w_f != 0.0 && !f_ref) return fail(h, NNP_ERR_ARG, "f_ref is required when w_f is nonzero");
+    if (!(w_f >= 0.0)) return fail(h, NNP_ERR_ARG, "w_f must be non-negative");
+    if (norm_mode < 0 || norm_mode > 4) return fail(h, NNP_ERR_ARG, "unknown norm mode");
+    const int S = batch->n_struct;
+    if (S <= 0) return fail(h, NNP_ERR_ARG, "empty batch");
+    if (w_f != 0.0)
+        for (const auto &net : E.host.nets)
+            if (net.neuron != nnp::NEU_LINEAR && net.neuron != nnp::NEU_SIGMOID && net.neuron != nnp::NEU_TANH)
+                return fail(h, NNP_ERR_UNSUPPORTED, "the force term needs f'' of the activation (LINEAR, SIGMOID or TANH)");
+    // forward: energies (no vacuum terms, as nnptefr subtracts them from the labels) and forces
+    const int64_t N = batch->atom_off[S];
+    std::vector<double> Eh(S), Fh((size_t)std::max<int64_t>(N, 1) * 3);
+    int rc = nnp_compute(h, batch, Eh.data(), Fh.data(), nullptr, NNP_ENERGY | NNP_FORCES);
+    if (rc != NNP_OK) return rc;
+    // loss and the per-structure / per-atom factors (nnptefr.cpp:614-620 norms)
+    std::vector<float> ge((size_t)std::max<int64_t>(N, 1));
+    std::vector<float4> tv((size_t)std::max<int64_t>(N, 1), make_float4(0.f, 0.f, 0.f, 0.f));
+    const double bi = 1.0 / S;
+    double L = 0.0;
+    for (int s = 0; s < S; ++s) {
+        const int64_t a0 = batch->atom_off[s], a1 = batch->atom_off[s + 1];
+        const double nat = (double)(a1 - a0);
+        double nrm = 1.0;
+        switch (norm_mode) {
+        case 1: nrm = 1.0 / nat; break;
+        case 2: nrm = 1.0 / std::sqrt(nat); break;
+        case 3: nrm = 1.0 / std::cbrt(nat); break;
+        case 4: nrm = 1.0 / (std::log(nat) + 1.0); break;
+        default: break;
+        }
+        const double dU = (Eh[s] - e_ref[s]) * nrm;
+        L += bi * 0.5 * dU * dU;
+        const double gf = nrm * dU * bi;
+        const double fs = nat > 0 ? w_f / (3.0 * nat) : 0.0;
+        double lf = 0.0;
+        for (int64_t a = a0; a < a1; ++a) {
+            ge[a] = (float)gf;
+            if (w_f != 0.0) {
+                double d[3];
+                for (int k = 0; k < 3; ++k) {
+                    d[k] = Fh[3 * a + k] - f_ref[3 * a + k];
+                    lf += d[k] * d[k];
+                }
+                tv[a] = make_float4((float)(fs * d[0] * bi), (float)(fs * d[1] * bi), (float)(fs * d[2] * bi), 0.f);
+            }
+        }
+        L += bi * 0.5 * fs * lf;
+    }
+    cudaError_t ce = cudaSuccess;
+    auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
+    chk(E.gE.reserve(std::max<int64_t>(N, 1)));
+    chk(E.pgrad.reserve(E.wfloats));
+    if (w_f != 0.0) {
+        chk(E.tvec.reserve(std::max<int64_t>(N, 1)));
+        chk(E.tang.reserve((size_t)std::max<int64_t>(N, 1) * E.gstride));
+    }
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
+    chk(cudaMemcpyAsync(E.gE.p, ge.data(), sizeof(float) * N, cudaMemcpyHostToDevice, E.stream));
+    if (w_f != 0.0) chk(cudaMemcpyAsync(E.tvec.p, tv.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("copy failed: ") + cudaGetErrorString(ce));
+    std::string msg = nnp::run_train_grad(E, w_f != 0.0);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    std::vector<double> gw((size_t)E.wfloats);
+    chk(cudaMemcpyAsync(gw.data(), E.pgrad.p, sizeof(double) * E.wfloats, cudaMemcpyDeviceToHost, E.stream));
+    chk(cudaStreamSynchronize(E.stream));
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("gradient failed: ") + cudaGetErrorString(ce));
+    // wpar layout -> reference packing (biases by layer, then column-major weights)
+    size_t k = 0;
+    for (int t = 0; t < E.dpot.ntypes; ++t) {
+        const nnp::DevType &T = E.dpot.t[t];
+        const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+        int64_t off = T.woff + 2 * nin + 2 * nout;
+        std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
+        for (int l = 0; l < T.nlayer; ++l) {
+            boff[l] = off;
+            woff[l] = off + T.nodes[l + 1];
+            off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
+        }
+        for (int l = 0; l < T.nlayer; ++l)
+            for (int n = 0; n < T.nodes[l + 1]; ++n) grad[k++] = gw[boff[l] + n];
+        for (int l = 0; l < T.nlayer; ++l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) grad[k++] = gw[woff[l] + (int64_t)m * st + n];
+        }
+    }
+    *loss = L;
+    if (e_out) std::copy(Eh.begin(), Eh.end(), e_out);
+    if (f_out) std::copy(Fh.begin(), Fh.begin() + 3 * N, f_out);
+    return NNP_OK;
 }
 
 }  // extern "C"

@@ -840,6 +840,34 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
     }
 }
 
+// Network of one type in the packed float layout of wpar: inpw[nin],
+// inpb[nin], outw[nout], outb[nout], then per layer the bias[no] and the
+// transposed weights W^T[m * wt_stride(no) + n] = W[n][m].
+struct NetView {
+    const float *inpw, *inpb, *outw, *outb;
+    const float *b[NNP_MAX_LAYERS];
+    const float *wt[NNP_MAX_LAYERS];
+    int ws[NNP_MAX_LAYERS];   // row stride of W^T
+};
+
+__device__ inline NetView net_view(const float *base, const DevType &T)
+{
+    NetView v;
+    const float *p = base;
+    const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+    v.inpw = p; p += nin;
+    v.inpb = p; p += nin;
+    v.outw = p; p += nout;
+    v.outb = p; p += nout;
+    for (int l = 0; l < T.nlayer; ++l) {
+        const int ni = T.nodes[l], no = T.nodes[l + 1];
+        v.b[l] = p; p += no;
+        v.ws[l] = wt_stride(no);
+        v.wt[l] = p; p += (i64)ni * v.ws[l];
+    }
+    return v;
+}
+
 // Prebuilt path: every angular block goes through the generic code above.
 struct GenericBlocks {
     template <typename Acc>

@@ -92,6 +92,11 @@ struct Engine {
     DBuf<float> G, dEdG, e_atom;
     DBuf<double> e_struct, force, symm_d;
     DBuf<DevErr> err;
+    // training (nnp_train_grad)
+    DBuf<float4> tvec;            // per-atom force factor V_i (x, y, z, 0)
+    DBuf<float> gE;               // per-atom energy factor
+    DBuf<float> tang;             // tangent symmetry functions C [N * gstride]
+    DBuf<double> pgrad;           // parameter gradient in the wpar layout [wfloats]
     DevErr *h_err = nullptr;      // pinned
     // pinned staging for host-pointer calls
     void *h_stage = nullptr;
@@ -124,6 +129,7 @@ std::string run_energy(Engine &E, bool vacuum);
 std::string run_symm_to_double(Engine &E, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
+std::string run_train_grad(Engine &E, bool with_force);
 std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,
                                     const float *G, int gstride, bool vacuum, double *energy);
 

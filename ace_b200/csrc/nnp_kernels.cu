@@ -407,32 +407,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
 
 // ------------------------------------------------------------------ networks (FP32)
 
-// Network of type t in shared memory, layout of nnp_internal.h (net_floats).
-struct NetView {
-    const float *inpw, *inpb, *outw, *outb;
-    const float *b[NNP_MAX_LAYERS];
-    const float *wt[NNP_MAX_LAYERS];
-    int ws[NNP_MAX_LAYERS];   // row stride of W^T
-};
-
-__device__ inline NetView net_view(const float *base, const DevType &T)
-{
-    NetView v;
-    const float *p = base;
-    const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
-    v.inpw = p; p += nin;
-    v.inpb = p; p += nin;
-    v.outw = p; p += nout;
-    v.outb = p; p += nout;
-    for (int l = 0; l < T.nlayer; ++l) {
-        const int ni = T.nodes[l], no = T.nodes[l + 1];
-        v.b[l] = p; p += no;
-        v.ws[l] = wt_stride(no);
-        v.wt[l] = p; p += (int64_t)ni * v.ws[l];
-    }
-    return v;
-}
-
 // One warp per atom: forward pass, atomic energy, and the input gradient
 // dE/dG = outw d_L W_L ... d_0 W_0 diag(inpw) (DODZ::grad).
 __global__ void __launch_bounds__(WARPS * 32) k_nn_fp32(int64_t N, const DevPot *__restrict__ pot,
