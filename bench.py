@@ -1,8 +1,8 @@
 #!/usr/bin/env python
 """NNP energy+force throughput (atoms/s) on B200.
 
-Workload (per GPU, weak scaling): the batched-inference configuration --
-4096 periodic structures with 16-512 atoms (uniform), 3 elements with
+Default workload (per GPU, weak scaling): batched inference -- 4096
+periodic structures with 16-512 atoms (uniform), 3 elements with
 Dirichlet(1,1,1) fractions, triclinic cells at 0.05 atoms/A^3 with +-10%
 shear, cutoff 6 A, per element 24 radial + 32 angular symmetry functions
 and a 56-32-32-1 tanh network.  Synthetic, seeded (no public dataset exists).
@@ -16,6 +16,11 @@ symmetry functions, networks, forces, per-structure energies.
           host->device copy of the inputs and the device->host copy of the
           energies and forces inside the timed region (wall clock).
 
+Other workloads (--workload): small (one 64-atom cell), train (energy+force
+loss gradient of 256 structures), large (one 131,072-atom FCC cell), stream
+(20,000 structures of 8-2048 atoms in batches of 1000, with per-batch
+latency percentiles).
+
 --impl reference times the reference's CPU implementation of the path on
 this host's cores (the reference's own code compiled in oracle/_ref, else
 the FP64 restatement in oracle/), on a bounded sample of the same workload.
@@ -24,7 +29,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -39,7 +43,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "NNP energy+force atoms/s on 1 B200, plain vs batched+BF16, at stated force error"
 UNIT = "atoms/s"
-WORKLOAD = "batched inference: 4096 structures x U{16..512} atoms, 3 elements, 56-32-32-1 tanh, rc 6 A"
+
+WORKLOADS = {
+    "batched": (2, "batched inference: 4096 structures x U{16..512} atoms, 3 elements, 56-32-32-1 tanh, rc 6 A"),
+    "small": (1, "one 64-atom single-element cubic cell (8.5 A), 16+16 functions, 32-20-20-1 tanh, rc 6 A"),
+    "train": (3, "training step: 256 structures x U{64..256} atoms, 2 elements, 48-32-32-1 tanh, "
+                 "energy+force MSE loss gradient (w_f 1, norm LINEAR)"),
+    "large": (4, "one 131,072-atom jittered FCC cell (a 4.05 A, 32^3 cells), 2 elements, 80-64-64-1 tanh, rc 6.5 A"),
+    "stream": (5, "20,000 structures, log-uniform 8..2048 atoms, 4 elements, 64-48-48-1 tanh, batches of 1000 "
+                  "structures"),
+}
+STREAM_BATCH = 1000
 
 
 def parse():
@@ -48,31 +62,49 @@ def parse():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--structures", type=int, default=4096)
+    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS))
+    ap.add_argument("--structures", type=int, default=4096, help="structures per GPU (batched workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
-# ---------------------------------------------------------------- workload
+# ---------------------------------------------------------------- workloads
 
-def workload(rank: int, n_struct: int):
+def make_batch(name: str, rank: int, n_struct: int = 4096):
     from ace_b200 import synth
-    return synth.config2(seed=11 + 1000 * rank, n_struct=n_struct)
+    if name == "batched":
+        return synth.config2(seed=11 + 1000 * rank, n_struct=n_struct)
+    if name == "small":
+        return synth.config1(seed=7 + 1000 * rank)
+    if name == "train":
+        return synth.config3(seed=13 + 1000 * rank)
+    if name == "large":
+        return synth.config4(seed=17 + 1000 * rank)
+    return synth.config5(seed=19 + 1000 * rank)
 
 
-def conditioning_sample():
+def conditioning_sample(name: str):
+    """Structures whose symmetry-function statistics set each network's input
+    bias/scale (nnptefr's PREBIAS MEAN / PRESCALE DEV)."""
     from ace_b200 import synth
-    return synth.config2(seed=999, n_struct=16)
+    if name == "batched":
+        return synth.config2(seed=999, n_struct=16)
+    if name == "small":
+        return synth.config1()
+    if name == "train":
+        return synth.config3(seed=998, n_struct=16)
+    if name == "large":
+        return synth.config4(seed=997, ncell=8)
+    return synth.config5(seed=996, n_struct=32)
 
 
-def build_potential(path: str):
-    """Config-2 potential; input bias/scale from G statistics of a 16-structure
-    sample computed by the GPU path (nnptefr's PREBIAS MEAN / PRESCALE DEV)."""
+def build_potential(name: str, path: str, seed: int = 1234):
+    """The workload's potential, conditioned on G computed by the GPU path."""
     from ace_b200 import NNP, potential, synth
-    pot = synth.potential_config(2)
+    pot = synth.potential_config(WORKLOADS[name][0], seed=seed)
     potential.write(path, pot)
     nn = NNP.read(path)
-    s = conditioning_sample()
+    s = conditioning_sample(name)
     _, _, G = nn.compute_batch(s.atom_off, s.pos, s.type, s.cell, symm=True)
     nn.close()
     synth.condition(pot, G, s.type)
@@ -110,6 +142,16 @@ def flops_per_stage(pot, types: np.ndarray, counts: np.ndarray):
         nodes = pot.nets[II].nodes
         f_nn += len(c) * 4 * sum(nodes[l] * nodes[l + 1] for l in range(len(nodes) - 1))
     return {"symm": f_symm, "forces": f_force, "networks": f_nn, "pairs": pairs, "triplets": trip}
+
+
+# DRAM bytes per atom of one launch, from the ncu capture of the 512-structure
+# case of the batched workload (dram__bytes_read.sum + dram__bytes_write.sum / atoms)
+DRAM_BYTES_PER_ATOM = {"k_force_jit": 145.647616e6 / 134400, "k_symm_jit": 118.50496e6 / 134400}
+
+
+def traffic_bytes(kernel: str, atoms: int):
+    b = DRAM_BYTES_PER_ATOM.get(kernel)
+    return None if b is None else round(b * atoms)
 
 
 # ---------------------------------------------------------------- clocks
@@ -188,16 +230,23 @@ def _ref_worker(args):
     return out
 
 
+def ref_kind():
+    """"reference" when the reference's own code is built in oracle/_ref."""
+    from oracle import ref
+    return "reference" if ref.available() else "port"
+
+
 def cpu_reference(path: str, batch, n_sample: int, procs: int):
     """Times the reference path (NeighborList::build + compute_symm +
     compute_force per structure, FP64) on n_sample structures with `procs`
     worker processes.  Returns (atoms/s, seconds, atoms, results)."""
     import multiprocessing as mp
     structs = [batch.structure(s) for s in range(min(n_sample, batch.n_struct))]
+    procs = max(1, min(procs, len(structs)))
     chunks = [structs[k::procs] for k in range(procs)]
     ctx = mp.get_context("spawn")
+    kind = ref_kind()
     with ctx.Pool(procs) as pool:
-        kind = ref_kind()
         pool.map(_ref_worker, [(path, [structs[0]], kind)] * procs)       # import / warm-up
         t0 = time.perf_counter()
         res = pool.map(_ref_worker, [(path, ch, kind) for ch in chunks])
@@ -210,23 +259,35 @@ def cpu_reference(path: str, batch, n_sample: int, procs: int):
     return atoms / dt, dt, atoms, ordered
 
 
-# DRAM bytes per atom of one launch, from the ncu capture of the 512-structure
-# case of this workload (dram__bytes_read.sum + dram__bytes_write.sum / atoms)
-DRAM_BYTES_PER_ATOM = {"k_force_jit": 145.647616e6 / 134400, "k_symm_jit": 118.50496e6 / 134400}
+def cpu_sample(name: str, b):
+    """Bounded CPU sample of the workload (about 10-30 s of CPU work) and its
+    description.  The large cell is replaced by a 4000-atom FCC cell of the
+    same density and basis: the reference's neighbour search is O(N^2) per
+    structure, its per-atom cost of the rest does not depend on N."""
+    from ace_b200 import synth
+    if name == "large":
+        return synth.config4(seed=17, ncell=10), "a 4000-atom FCC cell (10^3 cells) of the same density and basis"
+    if name == "small":
+        return b, "the 64-atom cell"
+    n = {"batched": 128, "stream": 64}[name]
+    s = b.subset(range(min(n, b.n_struct)))
+    return s, "first %d structures (%d atoms) of the rank-0 batch" % (s.n_struct, s.n_atoms)
 
 
-def traffic_bytes(kernel: str, atoms: int):
-    b = DRAM_BYTES_PER_ATOM.get(kernel)
-    return None if b is None else round(b * atoms)
+# ---------------------------------------------------------------- timing helpers
+
+def device_views(b, dev):
+    import torch
+    return (torch.tensor(b.atom_off, device=dev), torch.tensor(b.pos, device=dev),
+            torch.tensor(b.type, device=dev), torch.tensor(b.cell.reshape(-1, 9), device=dev))
 
 
-def ref_kind():
-    """"reference" when the reference's own code is built in oracle/_ref."""
-    from oracle import ref
-    return "reference" if ref.available() else "port"
+def pinned(a, dtype):
+    import torch
+    t_ = torch.empty(a.shape, dtype=dtype, pin_memory=True)
+    t_.numpy()[...] = a
+    return t_
 
-
-# ---------------------------------------------------------------- main
 
 def main():
     args = parse()
@@ -249,59 +310,83 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     from ace_b200 import NNP
+    name = args.workload
     tmp = tempfile.mkdtemp()
-    ppath = os.path.join(tmp, "config2.nnp")
-    pot = build_potential(ppath)
+    ppath = os.path.join(tmp, "potential.nnp")
+    pot = build_potential(name, ppath)
     nn = NNP.read(ppath)
     stream = torch.cuda.current_stream(dev)
     nn.set_stream(stream.cuda_stream)
+    b = make_batch(name, rank, args.structures)
+    clocks = ClockSampler(local)
+    if name == "train":
+        line = time_train(args, nn, b, ppath, world, dist, clocks, dev)
+    else:
+        line, E_chk, F_chk = time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            add_cpu_baseline(line, name, nn, b, ppath, E_chk, F_chk)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    nn.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
 
-    b = workload(rank, args.structures)
+
+def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
+    import torch
+    from ace_b200 import NNP
     N, S = b.n_atoms, b.n_struct
-    off = torch.tensor(b.atom_off, device=dev)
-    pos = torch.tensor(b.pos, device=dev)
-    typ = torch.tensor(b.type, device=dev)
-    cell = torch.tensor(b.cell.reshape(-1, 9), device=dev)
-    E = torch.zeros(S, dtype=torch.float64, device=dev)
-    F = torch.zeros(3 * N, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # calls: the whole batch, or the stream in pieces of STREAM_BATCH structures
+    pieces = [(0, S)] if name != "stream" else [(s, min(S, s + STREAM_BATCH)) for s in range(0, S, STREAM_BATCH)]
+    subs = [b.subset(range(s0, s1)) for s0, s1 in pieces] if len(pieces) > 1 else [b]
+    dviews = [device_views(sb, dev) for sb in subs]
+    outs = [(torch.zeros(sb.n_struct, dtype=torch.float64, device=dev),
+             torch.zeros(3 * sb.n_atoms, dtype=torch.float64, device=dev)) for sb in subs]
 
-    def step():
-        nn.compute_device(off.data_ptr(), pos.data_ptr(), typ.data_ptr(), cell.data_ptr(), S, E.data_ptr(),
-                          F.data_ptr())
+    def run_piece(k):
+        off, pos, typ, cell = dviews[k]
+        Eo, Fo = outs[k]
+        nn.compute_device(off.data_ptr(), pos.data_ptr(), typ.data_ptr(), cell.data_ptr(), subs[k].n_struct,
+                          Eo.data_ptr(), Fo.data_ptr())
 
     for _ in range(args.warmup):
-        step()
+        for k in range(len(subs)):
+            run_piece(k)
     torch.cuda.synchronize()
-    counts = nn.neighbor_counts(N)
-    fl = flops_per_stage(pot, b.type, counts)
+    cl = []
+    for k in range(len(subs)):          # neighbour counts of the whole workload
+        run_piece(k)
+        cl.append(nn.neighbor_counts(subs[k].n_atoms))
+    counts = np.concatenate(cl)
 
     # ---- device-resident timing
     nn.set_timing(True)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [[torch.cuda.Event(enable_timing=True) for _ in subs] for _ in range(args.steps)]
+    ends = [[torch.cuda.Event(enable_timing=True) for _ in subs] for _ in range(args.steps)]
     stage_ms = {k: 0.0 for k in NNP.STAGES}
-    clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = nn.launch_count()
     clocks.start()
-    for k in range(args.steps):
-        flush.zero_()
-        starts[k].record(stream)
-        step()
-        ends[k].record(stream)
-        st = nn.stage_times()
-        for key in stage_ms:
-            stage_ms[key] += st[key]
+    for i in range(args.steps):
+        for k in range(len(subs)):
+            flush.zero_()
+            starts[i][k].record(stream)
+            run_piece(k)
+            ends[i][k].record(stream)
+            st = nn.stage_times()
+            for key in stage_ms:
+                stage_ms[key] += st[key]
     torch.cuda.synchronize()
     clk = clocks.stop()
     launches = nn.launch_count() - launches0
     if world > 1:
         dist.barrier()
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    per_call = [s.elapsed_time(e) for i in range(args.steps) for s, e in zip(starts[i], ends[i])]
+    t = torch.tensor([sum(per_call)], dtype=torch.float64, device=dev)
     atoms = torch.tensor([float(N)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -312,25 +397,25 @@ def main():
     nn.set_timing(False)
 
     # ---- end to end through the C ABI with pinned host buffers
-    def pinned(a, dtype):
-        t_ = torch.empty(a.shape, dtype=dtype, pin_memory=True)
-        t_.numpy()[...] = a
-        return t_
-    h_off = pinned(b.atom_off, torch.int64)
-    h_pos = pinned(b.pos, torch.float64)
-    h_typ = pinned(b.type, torch.int32)
-    h_cell = pinned(b.cell.reshape(-1, 9), torch.float64)
-    h_E = torch.empty(S, dtype=torch.float64, pin_memory=True)
-    h_F = torch.empty((N, 3), dtype=torch.float64, pin_memory=True)
-    for _ in range(max(1, args.warmup)):
+    hsubs = [(pinned(sb.atom_off, torch.int64), pinned(sb.pos, torch.float64), pinned(sb.type, torch.int32),
+              pinned(sb.cell.reshape(-1, 9), torch.float64),
+              torch.empty(sb.n_struct, dtype=torch.float64, pin_memory=True),
+              torch.empty((sb.n_atoms, 3), dtype=torch.float64, pin_memory=True)) for sb in subs]
+
+    def run_host(k):
+        h_off, h_pos, h_typ, h_cell, h_E, h_F = hsubs[k]
         nn.compute_batch(h_off.numpy(), h_pos.numpy(), h_typ.numpy(), h_cell.numpy(), out_e=h_E.numpy(),
                          out_f=h_F.numpy())
+
+    for _ in range(max(1, args.warmup)):
+        for k in range(len(subs)):
+            run_host(k)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        nn.compute_batch(h_off.numpy(), h_pos.numpy(), h_typ.numpy(), h_cell.numpy(), out_e=h_E.numpy(),
-                         out_f=h_F.numpy())
+        for k in range(len(subs)):
+            run_host(k)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
@@ -338,34 +423,36 @@ def main():
     e2e_value = all_atoms * args.steps / float(te.item())
     h2d = b.atom_off.nbytes + b.pos.nbytes + b.type.nbytes + b.cell.nbytes
     d2h = S * 8 + N * 3 * 8
+    E_chk = np.concatenate([o[0].cpu().numpy() for o in outs])
+    F_chk = np.concatenate([o[1].cpu().numpy() for o in outs]).reshape(-1, 3)
 
     # ---- roofline of the dominant kernel (FP32 CUDA cores)
+    fl = flops_per_stage(pot, b.type, counts)
     per_step = {k: v / args.steps for k, v in stage_ms.items()}
     kern = max(("symm", "forces"), key=lambda k: per_step[k])
-    flo = fl[kern]
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_fp32 = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
-    achieved = flo / (per_step[kern] / 1e3) / 1e12
+    achieved = fl[kern] / (per_step[kern] / 1e3) / 1e12
     jit = bool(nn.specialization()[0])
     kname = ("k_symm" if kern == "symm" else "k_force") + ("_jit" if jit else "")
-    roofline = {"bound": "fp32", "kernel": kname,
-                "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak_fp32, 4),
-                "peak_source": "%d SMs x 128 FP32 FMA/clk x 2 x measured %.0f MHz (no FP32 figure in MEASURED_PEAKS.json)"
-                               % (n_sm, sm_mhz),
-                "traffic": traffic_bytes(kname, N)}
+    roofline = {"bound": "fp32", "kernel": kname, "achieved": round(achieved, 3), "peak": round(peak_fp32, 2),
+                "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
+                "peak_source": "%d SMs x 128 FP32 FMA/clk x 2 x measured %.0f MHz (no FP32 figure in "
+                               "MEASURED_PEAKS.json)" % (n_sm, sm_mhz),
+                "traffic": traffic_bytes(kname, N) if name == "batched" else None}
     if roofline["traffic"] is not None:
         roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one %s launch on the "
                                       "first 512 structures (134,400 atoms), scaled by atoms" % kname)
-
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "structures_per_gpu": S, "atoms_per_gpu": N,
-                   "pairs_per_atom": round(fl["pairs"] / N, 2), "triplets_per_atom": round(fl["triplets"] / N, 1),
-                   "l2": "flushed between timed steps (256 MB write, not timed)", "parallelism": "dp%d" % world},
+        "config": {"workload": WORKLOADS[name][1], "structures_per_gpu": S, "atoms_per_gpu": N,
+                   "pairs_per_atom": round(fl["pairs"] / max(N, 1), 2),
+                   "triplets_per_atom": round(fl["triplets"] / max(N, 1), 1),
+                   "l2": "flushed before every timed call (256 MB write, not timed)",
+                   "parallelism": "dp%d" % world},
         "stage_ms": {k: round(v, 4) for k, v in per_step.items()},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -373,58 +460,147 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if name == "stream":
+        line["batch_latency_ms"] = {"p50": round(float(np.percentile(per_call, 50)), 4),
+                                    "p99": round(float(np.percentile(per_call, 99)), 4),
+                                    "batches_per_step": len(subs), "structures_per_batch": STREAM_BATCH}
+    return line, E_chk, F_chk
 
-    # ---- CPU baseline (rank 0, one GPU only) and error against the FP64 oracle
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        procs = os.cpu_count() or 1
-        sample = b.subset(range(128))
-        v1, dt, at, res = cpu_reference(ppath, sample, 128, procs)
-        err_e, err_f = 0.0, 0.0
-        Eh = E.cpu().numpy()
-        Fh = F.cpu().numpy().reshape(-1, 3)
-        for s_ in range(sample.n_struct):
-            e_ref, f_ref = res[s_]
-            a0, a1 = int(b.atom_off[s_]), int(b.atom_off[s_ + 1])
-            err_e = max(err_e, abs(Eh[s_] - e_ref) / (a1 - a0))
-            err_f = max(err_f, float(np.abs(Fh[a0:a1] - f_ref).max()))
-        line["cpu_baseline"] = {"value": round(v1, 1), "unit": UNIT, "cores": procs, "kind": ref_kind(),
-                                "sample": "first 128 structures (%d atoms) of the rank-0 batch, %.1f s wall" % (at, dt)}
-        line["error_vs_fp64"] = {"energy_eV_per_atom_max": err_e, "force_eV_per_A_max": err_f,
-                                 "sample": "same 128 structures"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    nn.close()
+
+def add_cpu_baseline(line, name, nn, b, ppath, E_chk, F_chk):
+    """CPU baseline (rank 0, one GPU) and the error against the reference."""
+    procs = os.cpu_count() or 1
+    sample, desc = cpu_sample(name, b)
+    if name == "large":
+        Es, Fs = nn.compute_batch(sample.atom_off, sample.pos, sample.type, sample.cell)
+        Fs = Fs.reshape(-1, 3)
+    else:
+        Es, Fs = E_chk[:sample.n_struct], F_chk[:sample.n_atoms]
+    v1, dt, at, res = cpu_reference(ppath, sample, sample.n_struct, procs)
+    err_e, err_f = 0.0, 0.0
+    for s_ in range(sample.n_struct):
+        e_ref, f_ref = res[s_]
+        a0, a1 = int(sample.atom_off[s_]), int(sample.atom_off[s_ + 1])
+        err_e = max(err_e, abs(Es[s_] - e_ref) / (a1 - a0))
+        err_f = max(err_f, float(np.abs(Fs[a0:a1] - f_ref).max()))
+    line["cpu_baseline"] = {"value": round(v1, 1), "unit": UNIT, "cores": min(procs, sample.n_struct),
+                            "kind": ref_kind(), "sample": "%s, %.1f s wall" % (desc, dt)}
+    line["error_vs_fp64"] = {"energy_eV_per_atom_max": err_e, "force_eV_per_A_max": err_f, "sample": desc,
+                             "against": ref_kind()}
+
+
+def time_train(args, nn, b, ppath, world, dist, clocks, dev):
+    """Training step of configuration 3: nnp_train_grad on the batch (host
+    inputs and labels, forward + energy+force loss gradient, gradient copied
+    back), labels from a teacher potential plus noise (1 meV/atom, 20 meV/A)."""
+    import torch
+    from ace_b200 import NNP
+    tpath = os.path.join(os.path.dirname(ppath), "teacher.nnp")
+    build_potential("train", tpath, seed=4321)
+    teacher = NNP.read(tpath)
+    Et, Ft = teacher.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    teacher.close()
+    rng = np.random.default_rng(5)
+    nat = np.diff(b.atom_off)
+    e_ref = Et + rng.normal(0, 1e-3, size=b.n_struct) * nat
+    f_ref = Ft + rng.normal(0, 0.02, size=Ft.shape)
+    w_f = 1.0
+    for _ in range(args.warmup):
+        L, g, eo, fo = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, w_f, norm_mode=1)
+    torch.cuda.synchronize()
+    launches0 = nn.launch_count()
     if world > 1:
-        dist.destroy_process_group()
-    return 0
+        dist.barrier()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L, g, eo, fo = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, w_f, norm_mode=1)
+    dt = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = nn.launch_count() - launches0
+    t = torch.tensor([dt], dtype=torch.float64, device=dev)
+    atoms = torch.tensor([float(b.n_atoms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(atoms, op=dist.ReduceOp.SUM)
+    value = float(atoms.item()) * args.steps / float(t.item())
+    line = {"metric": METRIC + " (training step)", "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * float(t.item()) / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded teacher labels + noise)",
+            "config": {"workload": WORKLOADS["train"][1], "structures_per_gpu": b.n_struct,
+                       "atoms_per_gpu": b.n_atoms, "parallelism": "dp%d" % world,
+                       "timing": "wall clock around nnp_train_grad with host buffers (it synchronises); "
+                                 "value and e2e are the same measurement"},
+            "loss": L,
+            "e2e": {"value": round(value, 1), "unit": UNIT,
+                    "h2d_bytes_per_step": int(b.atom_off.nbytes + b.pos.nbytes + b.type.nbytes + b.cell.nbytes
+                                              + 20 * b.n_atoms),
+                    "d2h_bytes_per_step": int(8 * b.n_struct + 24 * b.n_atoms + 8 * len(g))},
+            "gpu_launches": int(launches), "clocks": clk}
+    if not args.no_cpu_baseline and world == 1:
+        import multiprocessing as mp
+        n = 16
+        sub = b.subset(range(n))
+        procs = max(1, min(os.cpu_count() or 1, n))
+        parts = [list(range(k, n, procs)) for k in range(procs)]
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            pool.map(_train_worker, [(ppath, sub, e_ref[:n], f_ref[:sub.n_atoms], [0])] * procs)
+            t0 = time.perf_counter()
+            pool.map(_train_worker, [(ppath, sub, e_ref[:n], f_ref[:sub.n_atoms], p) for p in parts])
+            dtc = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": round(sub.n_atoms / dtc, 1), "unit": UNIT, "cores": procs, "kind": "port",
+            "sample": ("FP64 restatement of the same energy+force loss gradient (orc_ef_loss_grad; the reference "
+                       "has no force-loss gradient), first %d structures (%d atoms), %.1f s wall"
+                       % (n, sub.n_atoms, dtc))}
+    return line
+
+
+def _train_worker(args):
+    path, sub, e_ref, f_ref, idx = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    op = orc.OraclePot.from_file(path)
+    for s in idx:
+        one = sub.subset([s])
+        a0, a1 = int(sub.atom_off[s]), int(sub.atom_off[s + 1])
+        orc.ef_loss_grad(op, one, e_ref[s:s + 1], f_ref[a0:a1], 1.0, norm_mode=1)
+    return True
 
 
 def run_reference(args, world):
     """CPU reference arm: each step evaluates a bounded sample of the workload."""
     from ace_b200 import potential, synth
+    name = args.workload
     tmp = tempfile.mkdtemp()
-    ppath = os.path.join(tmp, "config2.nnp")
-    pot = synth.potential_config(2)
+    ppath = os.path.join(tmp, "potential.nnp")
+    pot = synth.potential_config(WORKLOADS[name][0])
     potential.write(ppath, pot)
-    b = workload(0, args.structures)
+    b = make_batch(name, 0, args.structures)
+    if name == "large":
+        b = synth.config4(seed=17, ncell=10)
     procs = os.cpu_count() or 1
-    sample_structs = 64
+    per_step = {"batched": 64, "small": 1, "train": 16, "large": 1, "stream": 32}[name]
     times, atoms = [], 0
     for k in range(args.warmup + args.steps):
-        sub = b.subset(range((k * sample_structs) % b.n_struct, (k * sample_structs) % b.n_struct + sample_structs))
-        v, dt, at, _ = cpu_reference(ppath, sub, sample_structs, procs)
+        s0 = (k * per_step) % b.n_struct
+        sub = b.subset(range(s0, min(b.n_struct, s0 + per_step)))
+        v, dt, at, _ = cpu_reference(ppath, sub, sub.n_struct, procs)
         if k >= args.warmup:
             times.append(dt)
             atoms += at
     value = atoms / sum(times)
+    desc = ("%d structures per step" % per_step) if name != "large" else "a 4000-atom FCC cell per step"
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sample_per_step": "%d structures" % sample_structs,
+            "config": {"workload": WORKLOADS[name][1], "sample_per_step": desc,
                        "parallelism": "%d host processes" % procs},
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": procs, "kind": ref_kind(),
-                             "sample": "%d structures per step" % sample_structs},
+                             "sample": desc},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
