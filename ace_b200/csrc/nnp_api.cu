@@ -607,7 +607,6 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
     if ((flags & NNP_ENERGY) && !energy) return fail(h, NNP_ERR_ARG, "energy output missing");
     if ((flags & NNP_FORCES) && !forces) return fail(h, NNP_ERR_ARG, "force output missing");
     if ((flags & NNP_SYMM) && !symm_out) return fail(h, NNP_ERR_ARG, "symmetry-function output missing");
-    if (E.precision != NNP_PREC_FP32) return fail(h, NNP_ERR_UNSUPPORTED, "this build implements the FP32 network path only");
     const int S = b->n_struct;
     if (S == 0) return NNP_OK;
     if (!b->atom_off || !b->pos || !b->type || (b->pbc && !b->cell)) return fail(h, NNP_ERR_ARG, "batch array missing");
@@ -684,6 +683,7 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
             E.cap = std::min(NNP_MAX_NBR, ((er.need_cap + er.need_cap / 8 + 8) + 7) & ~7);
             continue;
         }
+        if (er.nonfinite == 2) { rc = fail(h, NNP_ERR_CUDA, "tensor-core network kernel: an MMA wait timed out"); break; }
         if (er.nonfinite) { rc = fail(h, NNP_ERR_NOT_FINITE, "non-finite energy or force"); }
         // outputs
         if (!devp) {
@@ -849,7 +849,11 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, c
     // forward: energies (no vacuum terms, as nnptefr subtracts them from the labels) and forces
     const int64_t N = batch->atom_off[S];
     std::vector<double> Eh(S), Fh((size_t)std::max<int64_t>(N, 1) * 3);
+    // the gradient kernels run the FP32 networks, so the forward pass does too
+    const int prec = E.precision;
+    E.precision = NNP_PREC_FP32;
     int rc = nnp_compute(h, batch, Eh.data(), Fh.data(), nullptr, NNP_ENERGY | NNP_FORCES);
+    E.precision = prec;
     if (rc != NNP_OK) return rc;
     // loss and the per-structure / per-atom factors (nnptefr.cpp:614-620 norms)
     std::vector<float> ge((size_t)std::max<int64_t>(N, 1));

@@ -683,6 +683,9 @@ std::string run_nn(Engine &E)
 {
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
+    // BF16 / split-BF16 tensor-core layers when every network fits them
+    if (E.precision != NNP_PREC_FP32 && tc_smem_bytes(E, E.precision == NNP_PREC_BF16X3) > 0)
+        return run_nn_tc(E, E.precision == NNP_PREC_BF16X3);
     const int maxn = max_nodes(E);
     const size_t sm = (size_t)(((E.wfloats + 3) & ~3) + WARPS * (NNP_MAX_LAYERS + 2) * maxn) * sizeof(float);
     if (sm > 220 * 1024) return "networks too large for the shared-memory FP32 path";

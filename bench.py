@@ -64,8 +64,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS))
     ap.add_argument("--structures", type=int, default=4096, help="structures per GPU (batched workload)")
+    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16", "bf16x3"],
+                    help="network layers: FP32 CUDA cores, or BF16 / split-BF16 tensor cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
+
+
+PRECISION = {"fp32": 0, "bf16": 1, "bf16x3": 2}
 
 
 # ---------------------------------------------------------------- workloads
@@ -315,6 +320,7 @@ def main():
     ppath = os.path.join(tmp, "potential.nnp")
     pot = build_potential(name, ppath)
     nn = NNP.read(ppath)
+    nn.set_precision(PRECISION[args.precision])
     stream = torch.cuda.current_stream(dev)
     nn.set_stream(stream.cuda_stream)
     b = make_batch(name, rank, args.structures)
@@ -447,8 +453,11 @@ def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32" if args.precision == "fp32" else "fp32 basis + %s networks" % args.precision,
+        "data": "synthetic (seeded)",
         "config": {"workload": WORKLOADS[name][1], "structures_per_gpu": S, "atoms_per_gpu": N,
+                   "network_precision": args.precision,
                    "pairs_per_atom": round(fl["pairs"] / max(N, 1), 2),
                    "triplets_per_atom": round(fl["triplets"] / max(N, 1), 1),
                    "l2": "flushed before every timed call (256 MB write, not timed)",
