@@ -546,12 +546,18 @@ __device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
 //    n*floor((n-1)/2) + (n even ? n/2 : 0) = n(n-1)/2 pairs.
 // Lanes step p by 32, which is (q32, r32) = (32/m, 32%m) in (g, f): two
 // adds and one wrap per step instead of a division or a square root.
+// The force kernel stores per-pair coefficients chunk by chunk: a J == K chunk
+// is NNP_PCH consecutive pairs (coefficient index p - c0); a J != K chunk is
+// whole rows a with row stride ps = nb (an odd padded stride, tried to avoid
+// bank conflicts between row owners, measured 2 % slower).
 struct Blk {
     int sa, na;       // first member: segment start / size
     int sb, nb;       // second member (sb == sa for J == K)
     bool tri;
     int npairs;
     int m, q32, r32;
+    int ps;           // coefficient row stride (J != K), see above
+    int chunk;        // pairs per force-kernel chunk
 };
 
 __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
@@ -566,6 +572,8 @@ __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
     k.m = k.nb;
     k.q32 = 32 / k.m;
     k.r32 = 32 - k.q32 * k.m;
+    k.ps = k.nb;                                         // nb < NNP_MAX_NBR <= NNP_PCH
+    k.chunk = k.tri ? NNP_PCH : (NNP_PCH / k.ps) * k.nb;
     return true;
 }
 
@@ -602,6 +610,13 @@ __device__ __forceinline__ void pit_slots(const Blk &k, const PairIt &it, int &a
         a = k.sa + it.g;
         b = k.sb + it.f;
     }
+}
+
+// coefficient index of the pair (p, it) in the force chunk that starts at pair
+// c0; row0 = c0 / nb is the chunk's first row (J != K chunks are whole rows)
+__device__ __forceinline__ int pc_index(const Blk &k, const PairIt &it, int p, int c0, int row0)
+{
+    return k.tri ? p - c0 : (it.g - row0) * k.ps + it.f;
 }
 
 // ---------------------------------------------------------------- generic block code
@@ -693,6 +708,7 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
 {
     const float *eb = v.vec + B.off_g;
     const bool gauss = (B.form == ANG_GAUSS);
+    const int row0 = k.tri ? 0 : c0 / k.nb;
     PairIt it = pit_init(k, c0 + lane);
 #pragma unroll 1
     for (int p = c0 + lane; p < c1; p += 32, pit_next(k, it)) {
@@ -745,7 +761,7 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 hrb = fmaf(ef, drb, hrb);
             }
         }
-        pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);
+        pair_coeffs(v.pc, pc_index(k, it, p, c0, row0), hc, hra, hrb, cs, ua.w, ub.w);
     }
 }
 
@@ -802,37 +818,32 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
         }
         return;
     }
+    // J != K: the chunk is rows [row0, row1), coefficient of (a, b) at
+    // (a - row0) * ps + b.  Row owners read with the odd stride ps across
+    // lanes (distinct banks), column owners consecutively.
+    // Row and column owners run the same loop (no divergent branches): slot
+    // sl walks its j-th pair with coefficient stride qs and partner stride us_.
+    const int row0 = c0 / k.nb, row1 = row0 + (c1 - c0) / k.nb;
     const int nslots = k.na + k.nb;
     for (int sl = lane; sl < nslots; sl += 32) {
         const bool is_row = sl < k.na;                 // first member of its pairs
         const int slot = is_row ? k.sa + sl : k.sb + (sl - k.na);
         const float4 us = v.u[slot];
         float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        if (is_row) {
-            const int rs = sl * k.nb;
-            const int p0 = max(rs, c0), p1 = min(rs + k.nb, c1);
-            for (int p = p0; p < p1; ++p) {
-                const float4 ub = v.u[k.sb + (p - rs)];
-                sa_ += cA[p - c0];
-                const float bt = cB[p - c0];
-                vx = fmaf(bt, ub.x, vx);
-                vy = fmaf(bt, ub.y, vy);
-                vz = fmaf(bt, ub.z, vz);
-            }
-        } else {
-            const int ic = sl - k.na;
-            // rows ra with c0 <= ra*nb + ic < c1 (c0 - ic > -nb, so the first quotient rounds up)
-            const int a0 = (c0 - ic + k.nb - 1) / k.nb;
-            const int a1 = (c1 - 1 - ic >= 0) ? min(k.na, (c1 - 1 - ic) / k.nb + 1) : 0;
-            for (int ra = a0; ra < a1; ++ra) {
-                const int p = ra * k.nb + ic;
-                const float4 ua = v.u[k.sa + ra];
-                sa_ += cC[p - c0];
-                const float dt = cD[p - c0];
-                vx = fmaf(dt, ua.x, vx);
-                vy = fmaf(dt, ua.y, vy);
-                vz = fmaf(dt, ua.z, vz);
-            }
+        const bool in_rows = sl >= row0 && sl < row1;
+        const int cnt = is_row ? (in_rows ? k.nb : 0) : row1 - row0;
+        const int q0 = is_row ? (sl - row0) * k.ps : sl - k.na;
+        const int qs = is_row ? 1 : k.ps;
+        const float *c1p = is_row ? cA : cC, *c2p = is_row ? cB : cD;
+        const float4 *up = v.u + (is_row ? k.sb : k.sa + row0);
+        for (int j = 0; j < cnt; ++j) {
+            const int q = q0 + j * qs;
+            const float4 uo = up[j];
+            sa_ += c1p[q];
+            const float bt = c2p[q];
+            vx = fmaf(bt, uo.x, vx);
+            vy = fmaf(bt, uo.y, vy);
+            vz = fmaf(bt, uo.z, vz);
         }
         v.gx[slot] += fmaf(sa_, us.x, vx);
         v.gy[slot] += fmaf(sa_, us.y, vy);
@@ -993,8 +1004,8 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             bool staged = false;
-            for (int c0 = 0; c0 < k.npairs; c0 += NNP_PCH) {
-                const int c1 = min(k.npairs, c0 + NNP_PCH);
+            for (int c0 = 0; c0 < k.npairs; c0 += k.chunk) {
+                const int c1 = min(k.npairs, c0 + k.chunk);
                 if (!Blocks::force(v, II, tt, k, c0, c1, cap, lane, v.vec + B.off_g)) {
                     if (!staged) {
                         for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
