@@ -101,6 +101,19 @@ __device__ __forceinline__ void store8(__nv_bfloat16 *hi, __nv_bfloat16 *lo, int
     if (lo) *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(l);
 }
 
+// Bias and transposed weights of layer l of a network in the wpar layout
+// (net_view's layout), found by walking the layers: no per-thread pointer
+// arrays, which the compiler would keep in local memory for a run-time l.
+__device__ __forceinline__ void layer_ptrs(const float *net, const DevType &T, int l, const float *&b, const float *&wt,
+                                           int &ws)
+{
+    const float *q = net + 2 * T.nodes[0] + 2 * T.nodes[T.nlayer];
+    for (int m = 0; m < l; ++m) q += T.nodes[m + 1] + (i64)T.nodes[m] * wt_stride(T.nodes[m + 1]);
+    b = q;
+    wt = q + T.nodes[l + 1];
+    ws = wt_stride(T.nodes[l + 1]);
+}
+
 // One MMA chain D[128 x N] = A[128 x K] * B[N x K]^T issued by thread 0 and
 // waited for by every thread.  Returns false when the wait gave up.
 __device__ bool gemm(const Smem &s, int a_off, int b_off, int K, int N, bool split, uint32_t tmem, uint32_t &phase)
@@ -177,16 +190,23 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
         TcPlan p;
         make_plan(DT, SPLIT, p);
         const Smem s = carve(smem_raw, p, SPLIT);
-        const NetView V = net_view(wpar + DT.woff, DT);
-        const int L = DT.nlayer, nin = DT.nodes[0];
+        const float *net = wpar + DT.woff;
+        const int L = DT.nlayer, nin = DT.nodes[0], nout = DT.nodes[L];
+        const float *inpw = net, *inpb = net + nin, *outw = net + 2 * nin, *outb = outw + nout;
+        const float *b_out, *w_out;
+        int ws_out;
+        layer_ptrs(net, DT, L - 1, b_out, w_out, ws_out);
         // ---- weights of this element in the operand layouts (zero padded)
         if (staged != T) {
             __syncthreads();
             for (int h = 0; h + 1 < L; ++h) {
-                const int ni = DT.nodes[h], no = DT.nodes[h + 1], Pi = p.P[h], Po = p.P[h + 1], ws = V.ws[h];
+                const int ni = DT.nodes[h], no = DT.nodes[h + 1], Pi = p.P[h], Po = p.P[h + 1];
+                const float *bh, *wth;
+                int ws;
+                layer_ptrs(net, DT, h, bh, wth, ws);
                 for (int q = t; q < Po * Pi; q += TILE) {
                     const int n = q / Pi, m = q - n * Pi;       // W[n][m], n < Po (out), m < Pi (in)
-                    const float w = (n < no && m < ni) ? V.wt[h][m * ws + n] : 0.f;
+                    const float w = (n < no && m < ni) ? wth[m * ws + n] : 0.f;
                     const __nv_bfloat16 hi = __float2bfloat16_rn(w);
                     s.w_hi[p.wf[h] + tc::kmaj(n, m, Pi)] = hi;
                     s.w_hi[p.wb[h] + tc::kmaj(m, n, Po)] = hi;
@@ -203,15 +223,22 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
         const int j = (g - first[T]) * TILE + t;
         const bool live = j < type_count[T];
         const i64 i = live ? order[base[T] + j] : 0;
-        // A_0 = inpw * (G + inpb), zero padded
+        // A_0 = inpw * (G + inpb), zero padded; the row is read as float4
+        // (gstride is a multiple of 4 and rows start 16-byte aligned), all of
+        // it before any use so the loads are in flight together
         {
             const float *Gi = G + i * gstride;
+#pragma unroll 4
             for (int k0 = 0; k0 < p.P[0]; k0 += 8) {
+                float4 lo4 = make_float4(0.f, 0.f, 0.f, 0.f), hi4 = lo4;
+                if (live && k0 + 4 <= gstride) lo4 = *reinterpret_cast<const float4 *>(Gi + k0);
+                if (live && k0 + 8 <= gstride) hi4 = *reinterpret_cast<const float4 *>(Gi + k0 + 4);
+                const float g[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
                 float v[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int k = k0 + q;
-                    v[q] = (live && k < nin) ? V.inpw[k] * (Gi[k] + V.inpb[k]) : 0.f;
+                    v[q] = (live && k < nin) ? inpw[k] * (g[q] + inpb[k]) : 0.f;
                 }
                 store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[0] + tc::kmaj(t, k0, p.P[0]), v);
             }
@@ -223,6 +250,9 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
             ok = gemm(s, p.tile[h], p.wf[h], p.P[h], Po, SPLIT, tmem, phase);
             if (!ok) break;
             const bool last = (h + 2 == L);
+            const float *bh, *wth;
+            int wsh;
+            layer_ptrs(net, DT, h, bh, wth, wsh);
             int doff = 0;
             for (int q = 0; q < h; ++q) doff += TILE * DT.nodes[q + 1];
             float *dh = s.d + doff;
@@ -236,13 +266,13 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                     out[q] = 0.f;
                     if (n < no) {
                         float a, d, d2;
-                        activation(DT.neuron, DT.c, z[q] + V.b[h][n], a, d, d2);
+                        activation(DT.neuron, DT.c, z[q] + bh[n], a, d, d2);
                         dh[n * TILE + t] = d;
                         if (last) {
                             // output layer: e = b + sum_n W[0][n] a_n; D = outw W[0][n] f'(z_n)
-                            const float wo = V.wt[L - 1][n * V.ws[L - 1]];
+                            const float wo = w_out[n * ws_out];
                             e = fmaf(wo, a, e);
-                            out[q] = V.outw[0] * wo * d;
+                            out[q] = outw[0] * wo * d;
                         } else {
                             out[q] = a;
                         }
@@ -252,7 +282,7 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                 // backward operand D_h in region h; both have K = P_{h+1}
                 store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[last ? h : h + 1] + tc::kmaj(t, c0, Po), out);
             }
-            if (last && live) e_atom[i] = V.outb[0] + (V.b[L - 1][0] + e) * V.outw[0];
+            if (last && live) e_atom[i] = outb[0] + (b_out[0] + e) * outw[0];
         }
         if (!ok) break;
         // ---- backward: D_{h-1} = (D_h W_h) * f'(z_{h-1}), dE/dG = (D_0 W_0) * inpw;
@@ -287,7 +317,7 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
                             const int n = c0 + q;
-                            if (n < gstride) o[n] = (n < nin) ? z[q] * V.inpw[n] : 0.f;
+                            if (n < gstride) o[n] = (n < nin) ? z[q] * inpw[n] : 0.f;
                         }
                     }
                 }
