@@ -67,7 +67,7 @@ void Engine::free_all()
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
     cell_pos.release(); order.release(); type_fill.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
-    e_struct.release(); force.release(); symm_d.release(); err.release();
+    e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
@@ -599,7 +599,14 @@ int nnp_set_params(nnp_handle *h, const double *params)
     return NNP_OK;
 }
 
-int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out, uint32_t flags)
+}  // extern "C"
+
+namespace {
+
+// nnp_compute and nnp_compute_md: the whole pipeline, with the optional
+// per-atom energies [N] and per-structure virials [9 S] of the MD call.
+int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out,
+                 double *atom_energy, double *virial, uint32_t flags)
 {
     if (!h || !b) return NNP_ERR_ARG;
     nnp::Engine &E = h->E;
@@ -660,13 +667,20 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
         E.type.p = const_cast<int32_t *>(b->type);
         E.cell.p = const_cast<double *>(b->cell);
     }
+    E.want_virial = (virial != nullptr);
+    if (virial) chk(E.vir.reserve(9 * (size_t)S));
+    if (atom_energy && !devp) chk(E.eatom_d.reserve(std::max<int64_t>(N, 1)));
+    if (ce != cudaSuccess) {
+        E.want_virial = false;
+        return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
+    }
     int rc = NNP_OK;
     for (int attempt = 0; attempt < 3; ++attempt) {
         std::string msg = nnp::run_prepare(E, N, S, b->pbc);
         if (msg.empty()) msg = nnp::run_neighbors(E, b->pbc);
         if (msg.empty()) msg = nnp::run_symm(E);
-        if (msg.empty() && (flags & (NNP_ENERGY | NNP_FORCES))) msg = nnp::run_nn(E);
-        if (msg.empty() && (flags & NNP_FORCES)) msg = nnp::run_force(E);
+        if (msg.empty() && ((flags & (NNP_ENERGY | NNP_FORCES)) || atom_energy || virial)) msg = nnp::run_nn(E);
+        if (msg.empty() && ((flags & NNP_FORCES) || virial)) msg = nnp::run_force(E);
         if (msg.empty() && (flags & NNP_ENERGY)) msg = nnp::run_energy(E, (flags & NNP_VACUUM) != 0);
         if (!msg.empty()) { rc = fail(h, NNP_ERR_CUDA, msg); break; }
         chk(cudaMemcpyAsync(E.h_err, E.err.p, sizeof(nnp::DevErr), cudaMemcpyDeviceToHost, E.stream));
@@ -695,10 +709,17 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
                 nnp::run_symm_to_double(E, E.symm_d.p);
                 chk(cudaMemcpyAsync(symm_out, E.symm_d.p, sizeof(double) * N * E.gstride, cudaMemcpyDeviceToHost, E.stream));
             }
+            if (atom_energy) {
+                nnp::run_atom_energy(E, (flags & NNP_VACUUM) != 0, E.eatom_d.p);
+                chk(cudaMemcpyAsync(atom_energy, E.eatom_d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, E.stream));
+            }
+            if (virial) chk(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost, E.stream));
         } else {
             if (flags & NNP_ENERGY) chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToDevice, E.stream));
             if (flags & NNP_FORCES) chk(cudaMemcpyAsync(forces, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, E.stream));
             if (flags & NNP_SYMM) nnp::run_symm_to_double(E, symm_out);
+            if (atom_energy) nnp::run_atom_energy(E, (flags & NNP_VACUUM) != 0, atom_energy);
+            if (virial) chk(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9 * S, cudaMemcpyDeviceToDevice, E.stream));
         }
         chk(cudaStreamSynchronize(E.stream));
         if (ce != cudaSuccess) rc = fail(h, NNP_ERR_CUDA, std::string("output copy failed: ") + cudaGetErrorString(ce));
@@ -710,7 +731,27 @@ int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *force
         E.cell = u_cell;
         E.type = u_type;
     }
+    E.want_virial = false;
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nnp_compute(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out, uint32_t flags)
+{
+    return compute_impl(h, b, energy, forces, symm_out, nullptr, nullptr, flags);
+}
+
+int nnp_compute_md(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *atom_energy,
+                   double *virial, uint32_t flags)
+{
+    if (!h || !b) return NNP_ERR_ARG;
+    if (flags & ~(uint32_t)(NNP_VACUUM | NNP_DEVICE_PTRS)) return fail(h, NNP_ERR_ARG, "flags other than NNP_VACUUM and NNP_DEVICE_PTRS");
+    if (!energy && !forces && !atom_energy && !virial) return fail(h, NNP_ERR_ARG, "no output requested");
+    flags |= (energy ? NNP_ENERGY : 0u) | (forces ? NNP_FORCES : 0u);
+    return compute_impl(h, b, energy, forces, nullptr, atom_energy, virial, flags);
 }
 
 int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, const int64_t *d_atom_off,

@@ -964,7 +964,8 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
                            const float4 *__restrict__ apar, const int *__restrict__ type, const int *__restrict__ order,
                            const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, int ncut_max,
                            int ndamp_max, int gstride, const float *__restrict__ dEdG, double *__restrict__ F,
-                           DevErr *err, float *smem)
+                           DevErr *err, float *smem, const int *__restrict__ atom_struct = nullptr,
+                           double *__restrict__ vir = nullptr)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
@@ -1041,6 +1042,28 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             atomicAdd(&F[3 * i], -fx);
             atomicAdd(&F[3 * i + 1], -fy);
             atomicAdd(&F[3 * i + 2], -fz);
+        }
+        if (vir) {
+            // virial W = -dE/d(strain): under x -> (I + e) x every displacement
+            // d_k = x_i - x_j - R q becomes (I + e) d_k, so W_ab = -sum_k g_a d_b
+            double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int k = lane; k < n; k += 32) {
+                const double g3[3] = {v.gx[k], v.gy[k], v.gz[k]};
+                const float4 u = v.u[k];
+                const double r = v.r[k];
+                const double d3[3] = {u.x * r, u.y * r, u.z * r};
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) w[3 * a + b] -= g3[a] * d3[b];
+            }
+#pragma unroll
+            for (int q = 0; q < 9; ++q) w[q] = warp_sum(w[q]);
+            if (lane == 0) {
+                double *ws = vir + 9 * (i64)atom_struct[i];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) atomicAdd(ws + q, w[q]);
+            }
         }
         if (__any_sync(NNP_FULL, bad) && lane == 0) atomicMax(&err->nonfinite, 1);
         __syncwarp();

@@ -92,6 +92,9 @@ struct Engine {
     DBuf<float> G, dEdG, e_atom;
     DBuf<double> e_struct, force, symm_d;
     DBuf<DevErr> err;
+    DBuf<double> vir;             // per-structure virial [9 * S] (when want_virial)
+    DBuf<double> eatom_d;         // per-atom energies for host-pointer calls
+    bool want_virial = false;
     // training (nnp_train_grad)
     DBuf<float4> tvec;            // per-atom force factor V_i (x, y, z, 0)
     DBuf<float> gE;               // per-atom energy factor
@@ -127,6 +130,7 @@ std::string run_nn(Engine &E);
 std::string run_force(Engine &E);
 std::string run_energy(Engine &E, bool vacuum);
 std::string run_symm_to_double(Engine &E, double *out);
+std::string run_atom_energy(Engine &E, bool vacuum, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
 std::string run_train_grad(Engine &E, bool with_force);

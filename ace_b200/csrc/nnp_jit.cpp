@@ -293,11 +293,12 @@ k_force_jit(long long N, const nnp::DevPot *__restrict__ pot, const float2 *__re
             const float4 *__restrict__ apar, const int *__restrict__ type, const int *__restrict__ order,
            const float4 *__restrict__ nbr,
             const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max, int gstride,
-            const float *__restrict__ dEdG, double *__restrict__ F, nnp::DevErr *err)
+            const float *__restrict__ dEdG, double *__restrict__ F, nnp::DevErr *err,
+            const int *__restrict__ atom_struct, double *__restrict__ vir)
 {
     extern __shared__ float4 smem4[];
     nnp::force_body<nnp::JitBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, dEdG,
-                                    F, err, reinterpret_cast<float *>(smem4));
+                                    F, err, reinterpret_cast<float *>(smem4), atom_struct, vir);
 }
 )";
     return os.str();

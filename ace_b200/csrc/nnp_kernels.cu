@@ -485,11 +485,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot
                                                         const int *__restrict__ type, const int *__restrict__ order, const float4 *__restrict__ nbr,
                                                         const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
                                                         int gstride, const float *__restrict__ dEdG,
-                                                        double *__restrict__ F, DevErr *err)
+                                                        double *__restrict__ F, DevErr *err,
+                                                        const int *__restrict__ atom_struct, double *__restrict__ vir)
 {
     extern __shared__ float4 smem4[];
     force_body<GenericBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, dEdG, F, err,
-                              reinterpret_cast<float *>(smem4));
+                              reinterpret_cast<float *>(smem4), atom_struct, vir);
 }
 
 // ------------------------------------------------------------------ energies
@@ -702,6 +703,8 @@ std::string run_force(Engine &E)
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
     cudaMemsetAsync(E.force.p, 0, 3 * (size_t)N * sizeof(double), E.stream);
+    double *vir = E.want_virial ? E.vir.p : nullptr;
+    if (vir) cudaMemsetAsync(vir, 0, 9 * (size_t)E.n_struct * sizeof(double), E.stream);
     const size_t sm = view_bytes(E, true);
     const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
@@ -709,14 +712,15 @@ std::string run_force(Engine &E)
         long long n = N;
         int cap = E.cap, nc = ncut_max(E), nd = ndamp_max(E), gs = E.gstride;
         void *args[] = {&n, &E.d_pot, &E.rpar.p, &E.apar.p, &E.type.p, &E.order.p, &E.nbr.p, &E.nbr_cnt.p,
-                        &cap, &nc, &nd, &gs, &E.dEdG.p, &E.force.p, &E.err.p};
+                        &cap, &nc, &nd, &gs, &E.dEdG.p, &E.force.p, &E.err.p, &E.atom_struct.p, &vir};
         std::string msg = jit_launch(E.jit_force, grid, WARPS * 32, sm, E.stream, args);
         E.mark(4);
         return msg;
     }
     cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_force<<<grid, WARPS * 32, sm, E.stream>>>(N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.order.p, E.nbr.p, E.nbr_cnt.p, E.cap,
-                                                ncut_max(E), ndamp_max(E), E.gstride, E.dEdG.p, E.force.p, E.err.p);
+                                                ncut_max(E), ndamp_max(E), E.gstride, E.dEdG.p, E.force.p, E.err.p,
+                                                E.atom_struct.p, vir);
     E.mark(4);
     return cuda_msg("forces");
 }
@@ -729,6 +733,24 @@ std::string run_energy(Engine &E, bool vacuum)
     E.launches += 1;
     E.mark(5);
     return cuda_msg("energies");
+}
+
+// per-atom energies in FP64: the network energy of each atom, plus its
+// element's vacuum energy when requested (NNH::energy, nnh.cpp:207-210)
+__global__ void k_atom_energy(int64_t N, const float *__restrict__ e_atom, const int *__restrict__ type, int vacuum,
+                              const double *__restrict__ vac, double *__restrict__ out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < N) out[i] = (double)e_atom[i] + (vacuum ? vac[type[i]] : 0.0);
+}
+
+std::string run_atom_energy(Engine &E, bool vacuum, double *out)
+{
+    const int64_t N = E.n_atoms;
+    if (N == 0) return "";
+    k_atom_energy<<<grid_for(N, 256, 1 << 30), 256, 0, E.stream>>>(N, E.e_atom.p, E.type.p, vacuum ? 1 : 0, E.vac.p, out);
+    E.launches += 1;
+    return cuda_msg("per-atom energies");
 }
 
 std::string run_symm_to_double(Engine &E, double *out)

@@ -59,6 +59,7 @@ def lib():
             "nnp_rc": ([p, C.POINTER(d)], i),
             "nnp_n_input": ([p, i, C.POINTER(i)], i),
             "nnp_compute": ([p, C.POINTER(_Batch), p, p, p, u], i),
+            "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
             "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
             "nnp_nparams": ([p, i, C.POINTER(i)], i),
             "nnp_get_params": ([p, p], i),
@@ -247,6 +248,25 @@ class NNP:
         if symm:
             out.append(G[:N])
         return tuple(out)
+
+    def compute_md(self, atom_off, pos, types, cells, pbc=True, vacuum=False):
+        """nnp_compute_md: energies [n_struct], forces [N,3], per-atom energies
+        [N] and virials [n_struct,3,3] (W = -dE/d strain, eV)."""
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        S = len(atom_off) - 1
+        cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(S, 9) if pbc else None
+        N = int(atom_off[-1]) if S else 0
+        b = _Batch(S, atom_off.ctypes.data, pos.ctypes.data, types.ctypes.data,
+                   cells.ctypes.data if cells is not None else None, 1 if pbc else 0)
+        E = np.zeros(max(S, 1))
+        F = np.zeros((max(N, 1), 3))
+        A = np.zeros(max(N, 1))
+        W = np.zeros((max(S, 1), 3, 3))
+        self._check(lib().nnp_compute_md(self._h, C.byref(b), _ptr(E), _ptr(F), _ptr(A), _ptr(W),
+                                         VACUUM if vacuum else 0))
+        return E[:S], F[:N], A[:N], W[:S]
 
     def compute_device(self, atom_off_ptr: int, pos_ptr: int, type_ptr: int, cell_ptr: int, n_struct: int,
                        energy_ptr: int, force_ptr: int, pbc: bool = True, vacuum: bool = False):

@@ -136,6 +136,20 @@ int nnp_n_input(const nnp_handle *h, int32_t type, int32_t *n_input);
 int nnp_compute(nnp_handle *h, const nnp_batch *batch, double *energy, double *forces,
                 double *symm_out, uint32_t flags);
 
+/* Force call for molecular dynamics: nnp_compute plus the per-atom energies
+ * and the virial of every structure, the outputs a LAMMPS-style pair style needs
+ * (the reference's ML-ATOMNN pair style is not in its sources; its per-atom
+ * energy is NNH::energy, nnh.cpp:207-210).  Any output may be NULL.
+ *  energy[n_struct]      as nnp_compute
+ *  forces[3*N]           as nnp_compute
+ *  atom_energy[N]        network energy of each atom (plus its vacuum energy with NNP_VACUUM)
+ *  virial[9*n_struct]    W = -dE/d(strain), W[9s+3a+b] = -sum over pairs of
+ *                        (dE_i/dd)_a d_b for the displacements d = x_i - x_j - R q
+ *                        (eV; the pressure tensor is W / volume)
+ * flags: NNP_VACUUM, NNP_DEVICE_PTRS. */
+int nnp_compute_md(nnp_handle *h, const nnp_batch *batch, double *energy, double *forces, double *atom_energy,
+                   double *virial, uint32_t flags);
+
 /* Energy of every structure from precomputed symmetry functions; replaces
  * NNP::compute_energy (nnp.cpp:329-338) with NNH::energy (nnh.cpp:207-210):
  * sum over atoms of network(G) + vacuum energy.  symm is N*gstride (host). */
