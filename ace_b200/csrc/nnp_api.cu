@@ -69,6 +69,7 @@ void Engine::free_all()
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();
+    graph_release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
     d_pot = nullptr;
@@ -83,6 +84,14 @@ void Engine::free_all()
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : ev) e = nullptr;
+}
+
+void Engine::graph_release()
+{
+    if (graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)graph_exec);
+    graph_exec = nullptr;
+    graph_key.clear();
+    graph_launches = 0;
 }
 
 // Build the device potential.  Angular functions of one BasisA that form a
@@ -494,6 +503,14 @@ int nnp_specialization_check(const char *potential_path, char *log, int32_t log_
     return msg.empty() ? NNP_OK : NNP_ERR_CUDA;
 }
 
+int nnp_set_graphs(nnp_handle *h, int32_t enable)
+{
+    if (!h) return NNP_ERR_ARG;
+    h->E.graph_release();
+    h->E.use_graphs = enable != 0;
+    return NNP_OK;
+}
+
 int nnp_set_accumulation(nnp_handle *h, int32_t acc)
 {
     if (!h) return NNP_ERR_ARG;
@@ -675,13 +692,69 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
         return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
     }
     int rc = NNP_OK;
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    // the device-side step: every launch depends only on host-known sizes and
+    // the handle's buffers, so it can be captured as one CUDA graph
+    auto step = [&]() -> std::string {
         std::string msg = nnp::run_prepare(E, N, S, b->pbc);
         if (msg.empty()) msg = nnp::run_neighbors(E, b->pbc);
         if (msg.empty()) msg = nnp::run_symm(E);
         if (msg.empty() && ((flags & (NNP_ENERGY | NNP_FORCES)) || atom_energy || virial)) msg = nnp::run_nn(E);
         if (msg.empty() && ((flags & NNP_FORCES) || virial)) msg = nnp::run_force(E);
         if (msg.empty() && (flags & NNP_ENERGY)) msg = nnp::run_energy(E, (flags & NNP_VACUUM) != 0);
+        return msg;
+    };
+    // Graph replay: after a call has run eagerly (so every buffer has its
+    // size), the next call with the same key is captured once and then
+    // replayed.  Not on the legacy default stream (it cannot be captured),
+    // and not while the stage timers are on.
+    bool graphs = E.use_graphs && !E.timing && E.stream != nullptr && E.stream != cudaStreamLegacy &&
+                  E.stream != cudaStreamPerThread;
+    std::vector<int64_t> key;
+    if (graphs)
+        key = {N, S, b->pbc, E.cap, (int64_t)flags, (int64_t)(atom_energy != nullptr), (int64_t)(virial != nullptr),
+               E.precision, (int64_t)(intptr_t)(E.use_jit ? E.jit_symm : nullptr), (int64_t)E.acc64,
+               (int64_t)(intptr_t)E.atom_off.p,
+               (int64_t)(intptr_t)E.pos.p, (int64_t)(intptr_t)E.type.p, (int64_t)(intptr_t)E.cell.p,
+               (int64_t)(intptr_t)E.nbr.p, (int64_t)(intptr_t)E.G.p, (int64_t)(intptr_t)E.force.p,
+               (int64_t)(intptr_t)E.e_struct.p, (int64_t)(intptr_t)E.e_atom.p, (int64_t)(intptr_t)E.vir.p};
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::string msg;
+        if (graphs && E.graph_exec && key == E.graph_key) {
+            chk(cudaGraphLaunch((cudaGraphExec_t)E.graph_exec, E.stream));
+            E.launches += E.graph_launches;
+        } else if (graphs && key == E.graph_key) {
+            // second call with this key: capture, then replay
+            const int64_t l0 = E.launches;
+            cudaGraph_t graph = nullptr;
+            cudaError_t g = cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal);
+            if (g == cudaSuccess) {
+                msg = step();
+                g = cudaStreamEndCapture(E.stream, &graph);
+            }
+            cudaGraphExec_t exec = nullptr;
+            if (g == cudaSuccess && msg.empty()) g = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (g == cudaSuccess && msg.empty() && exec) {
+                E.graph_exec = exec;
+                E.graph_launches = E.launches - l0;
+                E.launches = l0;
+                chk(cudaGraphLaunch(exec, E.stream));
+                E.launches += E.graph_launches;
+            } else {
+                // capture not possible here: run eagerly from now on
+                cudaGetLastError();
+                if (exec) cudaGraphExecDestroy(exec);
+                E.use_graphs = false;
+                E.launches = l0;
+                msg = step();
+            }
+        } else {
+            if (graphs) {
+                E.graph_release();
+                E.graph_key = key;        // capture on the next call with this key
+            }
+            msg = step();
+        }
         if (!msg.empty()) { rc = fail(h, NNP_ERR_CUDA, msg); break; }
         chk(cudaMemcpyAsync(E.h_err, E.err.p, sizeof(nnp::DevErr), cudaMemcpyDeviceToHost, E.stream));
         chk(cudaStreamSynchronize(E.stream));
@@ -695,6 +768,9 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
                 break;
             }
             E.cap = std::min(NNP_MAX_NBR, ((er.need_cap + er.need_cap / 8 + 8) + 7) & ~7);
+            // the graph was made for the old capacity: drop it, retry eagerly
+            E.graph_release();
+            graphs = false;
             continue;
         }
         if (er.nonfinite == 2) { rc = fail(h, NNP_ERR_CUDA, "tensor-core network kernel: an MMA wait timed out"); break; }

@@ -109,6 +109,14 @@ struct Engine {
 
     // stage timers and launch counter
     bool timing = false;
+
+    // CUDA graph of the device-side step, replayed while the call's shape and
+    // device pointers repeat (see graph_key in nnp_api.cu)
+    bool use_graphs = true;
+    void *graph_exec = nullptr;     // cudaGraphExec_t
+    std::vector<int64_t> graph_key;
+    int64_t graph_launches = 0;     // kernels in the graph
+    void graph_release();
     cudaEvent_t ev[6] = {};
     int64_t launches = 0;
     void mark(int k)

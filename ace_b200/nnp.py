@@ -60,6 +60,7 @@ def lib():
             "nnp_n_input": ([p, i, C.POINTER(i)], i),
             "nnp_compute": ([p, C.POINTER(_Batch), p, p, p, u], i),
             "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
+            "nnp_set_graphs": ([p, i], i),
             "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
             "nnp_nparams": ([p, i, C.POINTER(i)], i),
             "nnp_get_params": ([p, p], i),
@@ -166,6 +167,10 @@ class NNP:
 
     def set_precision(self, prec: int):
         self._check(lib().nnp_set_precision(self._h, prec))
+
+    def set_graphs(self, on: bool = True):
+        """Replay the device-side step as a CUDA graph while calls repeat their shape."""
+        self._check(lib().nnp_set_graphs(self._h, 1 if on else 0))
 
     def set_accumulation(self, fp64: bool = True):
         """FP64 (default) or FP32 running sums of the symmetry functions."""

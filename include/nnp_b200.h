@@ -116,6 +116,15 @@ int nnp_specialization_check(const char *potential_path, char *log, int32_t log_
 /* Launch on this CUDA stream (cudaStream_t) instead of the handle's own one. */
 int nnp_set_stream(nnp_handle *h, void *cuda_stream);
 
+/* CUDA graphs (on by default; no reference counterpart, the reference runs on
+ * the CPU).  The device-side step of nnp_compute / nnp_compute_md -- neighbour
+ * list, symmetry functions, networks, forces, energies -- launches only
+ * kernels whose sizes the host knows, so when a call repeats the previous
+ * call's shape (atom and structure counts, flags, capacity, device buffers)
+ * the library captures the step once and then replays it as one graph, as in
+ * an MD loop.  Not used on the legacy default stream or with stage timers on. */
+int nnp_set_graphs(nnp_handle *h, int32_t enable);
+
 /* ---- inspection: NNP::ntypes / index / rc / NNH::nInput (nnp.hpp:78-87, nnh.hpp:140-142) ---- */
 int nnp_ntypes(const nnp_handle *h, int32_t *ntypes);
 int nnp_type_index(const nnp_handle *h, const char *name, int32_t *index);
