@@ -67,7 +67,7 @@ struct Engine {
     // kernels specialised for this potential at run time (nnp_jit.cpp)
     bool use_jit = true;
     void *jit_module = nullptr;   // cudaLibrary_t
-    void *jit_symm = nullptr, *jit_force = nullptr;   // cudaKernel_t
+    void *jit_symm = nullptr, *jit_force = nullptr, *jit_tangent = nullptr;   // cudaKernel_t
     std::string jit_source, jit_error;
 
     // stream / events

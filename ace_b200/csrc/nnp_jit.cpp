@@ -219,6 +219,58 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
     return os.str();
 }
 
+// Tangent of one GAUSS block's symmetry functions along the displacement
+// field (see tangent_body): per pair dG_f = zeta lf x^(zeta-1) w_a w_b dcos
+// + x^zeta (w'_a w_b rr_a + w_a w'_b rr_b), relative to the block's first
+// entry of the tangent row (Cb).
+std::string gen_tangent_body(const Engine &E, const DevBlockA &B)
+{
+    std::ostringstream os;
+    const std::vector<Fn> fs = block_fns(E, B);
+    os << "        {\n";
+    for (size_t f = 0; f < fs.size(); ++f) os << "            float s" << f << " = 0.f;\n";
+    os << "            PairIt it = pit_init(k, lane);\n"
+          "#pragma unroll 1\n"
+          "            for (int p = lane; p < k.npairs; p += 32, pit_next(k, it)) {\n";
+    std::ostringstream body;
+    std::vector<float> bases;
+    std::set<int> damps;
+    pair_prologue(body, fs, bases, damps, true);
+    body << "            const float rra = v.pc[a], rrb = v.pc[b];\n"
+            "            const float uba = ub.x * v.gx[a] + ub.y * v.gy[a] + ub.z * v.gz[a];\n"
+            "            const float uab = ua.x * v.gx[b] + ua.y * v.gy[b] + ua.z * v.gz[b];\n"
+            "            const float dcos = (uba - cs * rra) * ua.w + (uab - cs * rrb) * ub.w;\n";
+    for (int d : damps) {
+        body << "            const float W" << d << " = wa" << d << " * wb" << d << " * dcos;\n";
+        body << "            const float R" << d << " = fmaf(da" << d << " * wb" << d << ", rra, wa" << d << " * db" << d
+             << " * rrb);\n";
+    }
+    Powers P(body);
+    for (size_t f = 0; f < fs.size(); ++f) {
+        const Fn &g = fs[f];
+        const int b = base_of(bases, g.lf);
+        std::string pz, pm1;
+        if (g.iz >= 0) {
+            pz = P.pw(b, g.iz);
+            pm1 = (g.iz >= 1) ? P.pw(b, g.iz - 1) : "";
+        } else {
+            pm1 = P.power(b, g.zeta - 1.f, -1);
+            pz = "(" + pm1 + " * x" + std::to_string(b) + ")";
+        }
+        const std::string d = std::to_string(g.damp);
+        body << "            s" << f << " = fmaf(" << pz << ", R" << d << ", s" << f << ");\n";
+        if (!pm1.empty())
+            body << "            s" << f << " = fmaf(" << pm1 << ", " << flit(g.zeta * g.lf) << " * W" << d << ", s" << f
+                 << ");\n";
+    }
+    os << body.str() << "            }\n";
+    for (size_t f = 0; f < fs.size(); ++f) os << "            s" << f << " = warp_sum(s" << f << ");\n";
+    os << "            if (lane == 0) {\n";
+    for (size_t f = 0; f < fs.size(); ++f) os << "                Cb[" << f << "] = s" << f << ";\n";
+    os << "            }\n            return true;\n        }\n";
+    return os.str();
+}
+
 // switch cases of a dispatcher: keys with the same body share one case
 std::string group_cases(const std::vector<std::pair<int, std::string>> &cases)
 {
@@ -259,7 +311,7 @@ std::string make_source(const Engine &E)
     os << "#define NNP_SYMM_MINB " << knob("NNP_SYMM_MINB", 3) << "\n#define NNP_FORCE_MINB "
        << knob("NNP_FORCE_MINB", 1) << "\n#define NNP_FORCE_UNROLL " << knob("NNP_FORCE_UNROLL", 1) << "\n";
     os << "#include \"nnp_device.cuh\"\nnamespace nnp {\nstruct JitBlocks {\n";
-    std::vector<std::pair<int, std::string>> sy, fo;
+    std::vector<std::pair<int, std::string>> sy, fo, ta;
     const int T = E.dpot.ntypes, TT = T * (T + 1) / 2;
     for (int II = 0; II < T; ++II)
         for (int tt = 0; tt < TT; ++tt) {
@@ -267,6 +319,7 @@ std::string make_source(const Engine &E)
             if (B.n == 0 || B.form != ANG_GAUSS) continue;
             sy.emplace_back(II * NNP_MAX_TT + tt, gen_symm_body(E, B));
             fo.emplace_back(II * NNP_MAX_TT + tt, gen_force_body(E, B));
+            ta.emplace_back(II * NNP_MAX_TT + tt, gen_tangent_body(E, B));
         }
     os << "    template <typename Acc>\n"
           "    __device__ static bool symm(const NbrView &v, int II, int tt, const Blk &k, int cap, int lane, float *Gb)\n"
@@ -275,7 +328,10 @@ std::string make_source(const Engine &E)
     os << "    __device__ static bool force(const NbrView &v, int II, int tt, const Blk &k, int c0, int c1, int cap,\n"
           "                                 int lane, const float *eb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
-       << group_cases(fo) << "        default: return false;\n        }\n    }\n};\n}  // namespace nnp\n";
+       << group_cases(fo) << "        default: return false;\n        }\n    }\n";
+    os << "    __device__ static bool tangent(const NbrView &v, int II, int tt, const Blk &k, int cap, int lane, float *Cb)\n"
+          "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
+       << group_cases(ta) << "        default: return false;\n        }\n    }\n};\n}  // namespace nnp\n";
     os << R"(
 extern "C" __global__ void __launch_bounds__(NNP_WARPS * 32, NNP_SYMM_MINB)
 k_symm_jit(long long N, const nnp::DevPot *__restrict__ pot, const float2 *__restrict__ rpar,
@@ -300,6 +356,17 @@ k_force_jit(long long N, const nnp::DevPot *__restrict__ pot, const float2 *__re
     nnp::force_body<nnp::JitBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, dEdG,
                                     F, err, reinterpret_cast<float *>(smem4), atom_struct, vir);
 }
+
+extern "C" __global__ void __launch_bounds__(NNP_WARPS * 32, 1)
+k_tangent_jit(long long N, const nnp::DevPot *__restrict__ pot, const float2 *__restrict__ rpar,
+              const float4 *__restrict__ apar, const int *__restrict__ type, const int *__restrict__ order,
+              const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, int ncut_max, int ndamp_max,
+              int gstride, const float4 *__restrict__ V, float *__restrict__ Cout)
+{
+    extern __shared__ float4 smem4[];
+    nnp::tangent_body<nnp::JitBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, V,
+                                      Cout, reinterpret_cast<float *>(smem4));
+}
 )";
     return os.str();
 }
@@ -310,7 +377,7 @@ void jit_release(Engine &E)
 {
     if (E.jit_module) cudaLibraryUnload((cudaLibrary_t)E.jit_module);
     E.jit_module = nullptr;
-    E.jit_symm = E.jit_force = nullptr;
+    E.jit_symm = E.jit_force = E.jit_tangent = nullptr;
 }
 
 std::string &jit_last_log()
@@ -425,9 +492,10 @@ std::string jit_build(Engine &E)
         cudaGetLastError();
         return "cudaLibraryLoadData failed";
     }
-    cudaKernel_t ks, kf;
+    cudaKernel_t ks, kf, kt;
     if (cudaLibraryGetKernel(&ks, lib, "k_symm_jit") != cudaSuccess ||
-        cudaLibraryGetKernel(&kf, lib, "k_force_jit") != cudaSuccess) {
+        cudaLibraryGetKernel(&kf, lib, "k_force_jit") != cudaSuccess ||
+        cudaLibraryGetKernel(&kt, lib, "k_tangent_jit") != cudaSuccess) {
         cudaGetLastError();
         cudaLibraryUnload(lib);
         return "run-time kernels not found";
@@ -435,6 +503,7 @@ std::string jit_build(Engine &E)
     E.jit_module = (void *)lib;
     E.jit_symm = (void *)ks;
     E.jit_force = (void *)kf;
+    E.jit_tangent = (void *)kt;
     return "";
 }
 

@@ -31,104 +31,8 @@ k_tangent(i64 N, const DevPot *__restrict__ pot, const float2 *__restrict__ rpar
           const float4 *__restrict__ V, float *__restrict__ Cout)
 {
     extern __shared__ float4 smem4[];
-    float *smem = reinterpret_cast<float *>(smem4);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
-    const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
-    // the force view's per-neighbour gradient arrays hold the relative
-    // displacement dv_k = V_i - V_k, and its pair-coefficient area the rate
-    // of change of the distance, rr_k = u_k . dv_k (cap <= NNP_MAX_NBR <= 4 NNP_PCH)
-    float *rr = v.pc;
-    const DevPot &P = *pot;
-    for (i64 idx = blockIdx.x * (i64)WARPS + warp; idx < N; idx += (i64)gridDim.x * WARPS) {
-        const i64 i = order[idx];
-        const int II = type[i];
-        const DevType &T = P.t[II];
-        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
-        const float4 vi = V[i];
-        for (int k = lane; k < n; k += 32) {
-            const float4 vk = V[v.j[k]];
-            const float dx = vi.x - vk.x, dy = vi.y - vk.y, dz = vi.z - vk.z;
-            v.gx[k] = dx;
-            v.gy[k] = dy;
-            v.gz[k] = dz;
-            const float4 u = v.u[k];
-            rr[k] = u.x * dx + u.y * dy + u.z * dz;
-        }
-        float *Ci = Cout + i * gstride;
-        for (int g = lane; g < gstride; g += 32) Ci[g] = 0.f;
-        __syncwarp();
-        // radial: dG/deps = G'(r) rr
-        for (int J = 0; J < P.ntypes; ++J) {
-            const DevBlockR B = T.br[J];
-            if (B.n == 0) continue;
-            const int s0 = v.seg[J], s1 = v.seg[J + 1];
-            for (int f = lane; f < B.n; f += 32) {
-                const float2 q = rpar[B.par + f];
-                float acc = 0.f;
-                for (int k = s0; k < s1; ++k) {
-                    float val, der;
-                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
-                    acc = fmaf(der, rr[k], acc);
-                }
-                Ci[B.off_g + f] = acc;
-            }
-        }
-        __syncwarp();
-        // angular: dG/deps = dG/dcos dcos + dG/dr_a rr_a + dG/dr_b rr_b with
-        // dcos = (u_b . dv_a - cos rr_a)/r_a + (u_a . dv_b - cos rr_b)/r_b
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
-            const DevBlockA B = T.ba[tt];
-            if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
-            Blk k;
-            if (!make_blk(v, J, K, k)) continue;
-            for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
-            __syncwarp();
-            for (int f0 = 0; f0 < B.n; f0 += NNP_SYMM_CHUNK) {
-                const int nf = min(NNP_SYMM_CHUNK, B.n - f0);
-                float acc[NNP_SYMM_CHUNK];
-#pragma unroll
-                for (int f = 0; f < NNP_SYMM_CHUNK; ++f) acc[f] = 0.f;
-                PairIt it = pit_init(k, lane);
-#pragma unroll 1
-                for (int p = lane; p < k.npairs; p += 32, pit_next(k, it)) {
-                    int a, b;
-                    pit_slots(k, it, a, b);
-                    const float4 ua = v.u[a], ub = v.u[b];
-                    const float cs = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
-                    const float uba = ub.x * v.gx[a] + ub.y * v.gy[a] + ub.z * v.gz[a];
-                    const float uab = ua.x * v.gx[b] + ua.y * v.gy[b] + ua.z * v.gz[b];
-                    const float ra = rr[a], rb = rr[b];
-                    const float dcos = (uba - cs * ra) * ua.w + (uab - cs * rb) * ub.w;
-                    const float fca = v.fc[B.cut * cap + a], fcb = v.fc[B.cut * cap + b];
-                    const float fda = v.fd[B.cut * cap + a], fdb = v.fd[B.cut * cap + b];
-#pragma unroll
-                    for (int f = 0; f < NNP_SYMM_CHUNK; ++f) {
-                        if (f < nf) {
-                            const float4 q = v.par[f0 + f];
-                            const int iz = (__float_as_int(q.w) >> 8) - 1;
-                            float h, hc, hra, hrb;
-                            angular_generic(B.form, v.r[a], v.r[b], cs, fca, fcb, fda, fdb, q.x, q.y, iz, q.z, true, h,
-                                            hc, hra, hrb);
-                            acc[f] = fmaf(hc, dcos, fmaf(hra, ra, fmaf(hrb, rb, acc[f])));
-                        }
-                    }
-                }
-#pragma unroll
-                for (int f = 0; f < NNP_SYMM_CHUNK; ++f) {
-                    if (f < nf) {
-                        const float s = warp_sum(acc[f]);
-                        if (lane == 0) Ci[B.off_g + f0 + f] = s;
-                    }
-                }
-            }
-            __syncwarp();
-        }
-        __syncwarp();
-    }
+    tangent_body<GenericBlocks>(N, pot, rpar, apar, type, order, nbr, nbr_cnt, cap, ncut_max, ndamp_max, gstride, V, Cout,
+                                reinterpret_cast<float *>(smem4));
 }
 
 // Per-warp work area of k_nn_train, in floats: per layer a, f', f'', the
@@ -288,13 +192,22 @@ std::string run_train_grad(Engine &E, bool with_force)
         const int per = nbr_view_floats(E.cap, ncut, ndamp, E.gstride, true);
         const size_t sm = (size_t)WARPS * ((per + 3) & ~3) * sizeof(float);
         if (sm > 227 * 1024) return "neighbour capacity too large for the tangent kernel";
-        cudaFuncSetAttribute(k_tangent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_tangent<<<grid_for(N, WARPS, nsm * 16), WARPS * 32, sm, E.stream>>>(
-            N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.order.p, E.nbr.p, E.nbr_cnt.p, E.cap, ncut, ndamp, E.gstride,
-            E.tvec.p, E.tang.p);
+        const int grid = grid_for(N, WARPS, nsm * 16);
         E.launches += 1;
-        std::string msg = cuda_msg("tangent symmetry functions");
-        if (!msg.empty()) return msg;
+        if (E.use_jit && E.jit_tangent) {
+            long long n = N;
+            int cap = E.cap, gs = E.gstride;
+            void *args[] = {&n, &E.d_pot, &E.rpar.p, &E.apar.p, &E.type.p, &E.order.p, &E.nbr.p, &E.nbr_cnt.p,
+                            &cap, &ncut, &ndamp, &gs, &E.tvec.p, &E.tang.p};
+            std::string msg = jit_launch(E.jit_tangent, grid, WARPS * 32, sm, E.stream, args);
+            if (!msg.empty()) return msg;
+        } else {
+            cudaFuncSetAttribute(k_tangent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_tangent<<<grid, WARPS * 32, sm, E.stream>>>(N, E.d_pot, E.rpar.p, E.apar.p, E.type.p, E.order.p, E.nbr.p,
+                                                          E.nbr_cnt.p, E.cap, ncut, ndamp, E.gstride, E.tvec.p, E.tang.p);
+            std::string msg = cuda_msg("tangent symmetry functions");
+            if (!msg.empty()) return msg;
+        }
     }
     const size_t sm = (size_t)(2 * ((E.wfloats + 3) & ~3) + WARPS * train_warp_floats(maxl, maxn)) * sizeof(float);
     if (sm > 227 * 1024) return "networks too large for the shared-memory training kernel";
