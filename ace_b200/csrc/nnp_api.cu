@@ -65,6 +65,7 @@ void Engine::free_all()
     atom_off.release(); pos.release(); cell.release(); xw.release();
     type.release(); atom_struct.release(); atom_cell.release(); grid.release();
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
+    cell_tcnt.release();
     cell_pos.release(); order.release(); type_fill.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();

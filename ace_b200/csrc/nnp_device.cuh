@@ -23,7 +23,7 @@
 
 #define NNP_WARPS 8           // warps per block of the per-atom kernels
 #define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
-#define NNP_PCH 256           // pairs per chunk of the force kernel's pair pass
+#define NNP_PCH 192           // pairs per chunk of the force kernel's pair pass
 #define NNP_FULL 0xffffffffu
 
 #ifdef __CUDACC__
@@ -443,6 +443,7 @@ struct NbrView {
     float4 *u;          // unit vector to the neighbour and inverse distance (ux, uy, uz, 1/r) [C]
     float *r;           // distance [C]
     float4 *par;        // block parameters [NNP_MAX_AFUNC]
+    float4 *raw;        // next atom's neighbour records, prefetched (force views) [C]
     int *j;             // neighbour atom index [C]
     float *fc, *fd;     // cutoff value / slope [ncut][C]
     float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr [ndamp][C]
@@ -456,7 +457,7 @@ struct NbrView {
 NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
 {
     return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 2 * ndamp * C +
-           (force ? 3 * C + gstride + 4 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+           (force ? 4 * C + 3 * C + gstride + 4 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
 __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
@@ -465,6 +466,11 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
     float *p = base;
     v.u = reinterpret_cast<float4 *>(p); p += 4 * C;                 // 16-byte aligned first
     v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
+    if (force) {
+        v.raw = reinterpret_cast<float4 *>(p); p += 4 * C;           // stays 16-byte aligned
+    } else {
+        v.raw = nullptr;
+    }
     v.r = p; p += C;
     v.j = reinterpret_cast<int *>(p); p += C;
     v.fc = p; p += ncut * C;
@@ -485,15 +491,15 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
     return v;
 }
 
-// Load atom i's neighbour list into the warp's view and compute the per-neighbour
+// Load an atom's neighbour list into the warp's view and compute the per-neighbour
 // quantities: unit vector, distance, cutoff value/slope per cutoff, and the
 // GAUSS damping factors w_e(r) = fc(r) exp(-a_e r^2) with slopes dw_e/dr.
-__device__ inline int stage_neighbors(const NbrView &v, i64 i, int cap, const float4 *__restrict__ nbr,
-                                      const int *__restrict__ nbr_cnt, const DevPot &P, const DevType &T, int lane)
+// (src: the atom's n neighbour records, in global or shared memory)
+__device__ __forceinline__ int stage_records(const NbrView &v, const float4 *src, int n, int cap, const DevPot &P,
+                                            const DevType &T, int lane)
 {
-    const int n = nbr_cnt[i];
     for (int k = lane; k < n; k += 32) {
-        const float4 e = nbr[i * cap + k];
+        const float4 e = src[k];
         const float r = sqrtf(e.x * e.x + e.y * e.y + e.z * e.z);
         const float ir = 1.f / r;
         v.u[k] = make_float4(e.x * ir, e.y * ir, e.z * ir, ir);
@@ -527,6 +533,41 @@ __device__ inline int stage_neighbors(const NbrView &v, i64 i, int cap, const fl
     }
     __syncwarp();
     return n;
+}
+
+// Asynchronous copy of n neighbour records (16 bytes each) into shared memory
+// (cp.async, completed by async_wait): the next atom's list streams in while
+// the warp works on the current one.
+__device__ __forceinline__ void prefetch_records(float4 *dst, const float4 *src, int n, int lane)
+{
+    for (int k = lane; k < n; k += 32) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + k);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + k) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// The per-atom kernels walk atoms idx, idx + stride, ... of the element-sorted
+// order.  prefetch_atom starts the copy of atom order[idx]'s records (if idx <
+// N) and returns its index and count; stage_prefetched waits for them and
+// stages them.
+__device__ __forceinline__ void prefetch_atom(const NbrView &v, i64 idx, i64 N, const int *__restrict__ order,
+                                              const float4 *__restrict__ nbr, const int *__restrict__ nbr_cnt,
+                                              int cap, int lane, i64 &i_next, int &n_next)
+{
+    if (idx < N) {
+        i_next = order[idx];
+        n_next = nbr_cnt[i_next];
+        prefetch_records(v.raw, nbr + i_next * cap, n_next, lane);
+    }
+}
+
+__device__ __forceinline__ int stage_prefetched(const NbrView &v, int n, int cap, const DevPot &P, const DevType &T,
+                                                int lane)
+{
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+    return stage_records(v, v.raw, n, cap, P, T, lane);
 }
 
 __device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
@@ -913,7 +954,7 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
         const i64 i = order[idx];
         const int II = type[i];
         const DevType &T = P.t[II];
-        stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        stage_records(v, nbr + i * cap, nbr_cnt[i], cap, P, T, lane);
         float *Gi = G + i * gstride;
         for (int g = lane; g < gstride; g += 32) Gi[g] = 0.f;
         __syncwarp();
@@ -972,11 +1013,16 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
     const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
     const DevPot &P = *pot;
-    for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
-        const i64 i = order[idx];
+    const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;
+    i64 i_next = 0;
+    int n_next = 0;
+    prefetch_atom(v, idx0, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
+    for (i64 idx = idx0; idx < N; idx += stride) {
+        const i64 i = i_next;
         const int II = type[i];
         const DevType &T = P.t[II];
-        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        const int n = stage_prefetched(v, n_next, cap, P, T, lane);
+        prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
         const float *e = dEdG + i * gstride;
         for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
         __syncwarp();
@@ -1091,11 +1137,16 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
     // of change of the distance, rr_k = u_k . dv_k (cap <= NNP_MAX_NBR <= 4 NNP_PCH)
     float *rr = v.pc;
     const DevPot &P = *pot;
-    for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
-        const i64 i = order[idx];
+    const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;
+    i64 i_next = 0;
+    int n_next = 0;
+    prefetch_atom(v, idx0, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
+    for (i64 idx = idx0; idx < N; idx += stride) {
+        const i64 i = i_next;
         const int II = type[i];
         const DevType &T = P.t[II];
-        const int n = stage_neighbors(v, i, cap, nbr, nbr_cnt, P, T, lane);
+        const int n = stage_prefetched(v, n_next, cap, P, T, lane);
+        prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
         const float4 vi = V[i];
         for (int k = lane; k < n; k += 32) {
             const float4 vk = V[v.j[k]];

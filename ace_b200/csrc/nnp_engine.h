@@ -84,6 +84,7 @@ struct Engine {
     DBuf<int> type, atom_struct, atom_cell;
     DBuf<StructGrid> grid;
     DBuf<int> cell_cnt, cell_start, cell_fill, cell_atoms, scan_tmp;
+    DBuf<int> cell_tcnt;          // members of each type per cell [cell][type]
     DBuf<double4> cell_pos;       // cell-ordered wrapped positions, type in .w
     DBuf<int> order;              // atoms grouped by element (visiting order of the per-atom kernels)
     DBuf<int> type_fill;          // [2 * NNP_MAX_TYPES] element counts and fill cursors

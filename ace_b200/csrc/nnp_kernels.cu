@@ -6,8 +6,9 @@
 //   k_cell_base    exclusive scan of cells per structure
 //   k_bin          wrap atoms into their cell, count atoms per cell
 //   k_cell_start   per-structure scan of the cell counts
-//   k_fill, k_sort_cells   cell member lists, sorted by atom index
-//   k_neigh        one warp per atom: candidates from the (2m+1)^3 cells,
+//   k_fill, k_sort_cells   cell member lists, sorted by type and atom index
+//   k_neigh        one block per cell: candidates from the (2m+1)^3 cells
+//                  gathered in shared memory, one warp per atom of the cell,
 //                  exact FP64 displacement test, neighbours grouped by type
 //                  (replaces NeighborList::build, struc/neighbor.cpp:46-87)
 //   k_symm         one warp per atom: radial + angular symmetry functions
@@ -247,22 +248,33 @@ __global__ void k_fill(int64_t N, const int *__restrict__ atom_cell, const int *
     cell_atoms[slot] = (int)i;
 }
 
-// one block per structure: insertion sort of every cell's member list, so the
-// neighbour order does not depend on the order of the atomic insertions
+// one block per structure: insertion sort of every cell's member list by
+// (type, atom index), so the neighbour order does not depend on the order of
+// the atomic insertions, and the count of each type among the members
 __global__ void k_sort_cells(const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
                              const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
-                             int *__restrict__ cell_atoms)
+                             const int *__restrict__ type, int ntypes, int *__restrict__ cell_atoms,
+                             int *__restrict__ cell_tcnt)
 {
     const int s = blockIdx.x;
     const int base = grid[s].cell_base, nc = ncells[s];
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
         int *a = cell_atoms + cell_start[base + k];
         const int n = cell_cnt[base + k];
+        for (int p = 0; p < n; ++p) a[p] |= type[a[p]] << 28;   // atom indices < 2^28, types < 8
         for (int p = 1; p < n; ++p) {
             const int v = a[p];
             int q = p - 1;
             while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
             a[q + 1] = v;
+        }
+        int *tc = cell_tcnt + (size_t)(base + k) * ntypes;
+        int p = 0;
+        for (int t = 0; t < ntypes; ++t) {
+            int q = p;
+            while (q < n && (a[q] >> 28) == t) a[q++] &= 0x0fffffff;
+            tc[t] = q - p;
+            p = q;
         }
     }
 }
@@ -278,113 +290,307 @@ __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const 
     cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2], (double)type[a]);
 }
 
-// one warp per atom.  Candidates are the members of the (2m+1)^3 cells around
-// the atom's cell, each with its lattice image shift; the FP64 displacement
-// x_i - (x_j + R q) decides membership (r^2 < rc^2; a self image needs
-// r^2 > 1e-12 as in neighbor.cpp:78).  The accepted list keeps candidate order
-// and is written grouped by neighbour type: float4(dx,dy,dz, j | type<<28).
-__global__ void __launch_bounds__(WARPS * 32, 3) k_neigh(int64_t N, const int *__restrict__ atom_struct,
-                                                     const int *__restrict__ atom_cell, const StructGrid *__restrict__ grid,
-                                                     const double *__restrict__ xw, const double4 *__restrict__ cell_pos,
-                                                     const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
-                                                     const int *__restrict__ cell_atoms, double rc2, int cap, int ntypes,
-                                                     float4 *__restrict__ nbr, int *__restrict__ nbr_cnt, DevErr *err)
+// Neighbour search, one thread block per cell.  Every atom of a cell has the
+// same candidates: the members of the (2m+1)^3 cells around it, each with its
+// lattice image shift.  The block gathers them into shared memory with the
+// shift applied in FP64 (x_j + R q), ordered by neighbour type, then by cell
+// offset, then by atom index (cell member lists are sorted by type and index),
+// and each warp tests one atom of the cell against the list: the FP64
+// displacement x_i - (x_j + R q) decides membership (r^2 < rc^2; a self image
+// needs r^2 > 1e-12 as in neighbor.cpp:78).  Accepted candidates are written
+// in list order, so each atom's list comes out grouped by type:
+// float4(dx,dy,dz, j | type<<28).  Candidate lists longer than the shared
+// buffer stream through it in chunks; a cell with more (type, cell) segments
+// than the segment table holds is searched from global memory, one warp per
+// atom, with the same order and arithmetic.
+#define NEIGH_THREADS (NNP_WARPS * 32)
+#define NEIGH_CAND 1536       // candidates held in shared memory at a time (multiple of 64)
+#define NEIGH_ENT 512         // (type, neighbouring cell) segments of one cell's candidate list
+#define NEIGH_ATOMS 1024      // atoms of one cell whose counts are kept while chunks stream
+
+struct NeighShared {
+    union {
+        struct {
+            double x[NEIGH_CAND], y[NEIGH_CAND], z[NEIGH_CAND];   // shifted candidate positions
+            int jt[NEIGH_CAND];                                  // j | type << 28
+        } c;
+        float4 lst[NNP_WARPS][NNP_MAX_NBR];   // global-memory search: accepted, j | type << 28 in .w
+    };
+    int count[NEIGH_ATOMS];                   // running neighbour counts (chunked lists)
+    int pre[NEIGH_ENT + 1];                   // exclusive scan of the segment lengths
+    int start[NEIGH_ENT];                     // first member slot of each segment
+    int q[NEIGH_ENT];                         // image shift of each segment, 3 x 8 bits
+};
+
+__device__ __forceinline__ int pack_q(int q0, int q1, int q2)
 {
-    __shared__ float4 s_lst[WARPS][NNP_MAX_NBR];
-    __shared__ int s_j[WARPS][NNP_MAX_NBR];
-    __shared__ unsigned char s_t[WARPS][NNP_MAX_NBR];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    return (q0 + 128) | ((q1 + 128) << 8) | ((q2 + 128) << 16);
+}
+
+// neighbouring cell o of local cell (c0,c1,c2): global index and image shift
+__device__ __forceinline__ int cell_offset(const StructGrid &g, int c0, int c1, int c2, int o, int &q0, int &q1, int &q2)
+{
+    const int w1 = 2 * g.m[1] + 1, w2 = 2 * g.m[2] + 1;
+    const int d2 = o % w2 - g.m[2];
+    const int t = o / w2;
+    const int d1 = t % w1 - g.m[1];
+    const int d0 = t / w1 - g.m[0];
+    const int t0 = c0 + d0, t1 = c1 + d1, t2 = c2 + d2;
+    q0 = floor_div(t0, g.nc[0]);
+    q1 = floor_div(t1, g.nc[1]);
+    q2 = floor_div(t2, g.nc[2]);
+    return g.cell_base + ((t0 - q0 * g.nc[0]) * g.nc[1] + (t1 - q1 * g.nc[1])) * g.nc[2] + (t2 - q2 * g.nc[2]);
+}
+
+// Candidates [k0, k1) of the cell's list into shared memory slots [0, k1-k0),
+// slots up to kp filled with NaN positions (never accepted).
+__device__ __forceinline__ void load_candidates(NeighShared &sh, int k0, int k1, int kp, int NE, const StructGrid &g,
+                                                const double4 *__restrict__ cell_pos,
+                                                const int *__restrict__ cell_atoms, int tid)
+{
+    const double R0 = g.R[0], R1 = g.R[1], R2 = g.R[2], R3 = g.R[3], R4 = g.R[4], R5 = g.R[5], R6 = g.R[6],
+                 R7 = g.R[7], R8 = g.R[8];
+    for (int s = tid; s < kp; s += NEIGH_THREADS) {
+        const int k = k0 + s;
+        if (k >= k1) {
+            const double nan = __longlong_as_double(0x7ff8000000000000ll);
+            sh.c.x[s] = sh.c.y[s] = sh.c.z[s] = nan;
+            sh.c.jt[s] = 0;
+            continue;
+        }
+        int lo = 0, hi = NE;                                     // last segment with pre <= k
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (sh.pre[mid] <= k) lo = mid; else hi = mid;
+        }
+        const int slot = sh.start[lo] + k - sh.pre[lo];
+        const double4 xj = cell_pos[slot];
+        const int j = cell_atoms[slot];
+        const int qp = sh.q[lo];
+        const double Q0 = (qp & 255) - 128, Q1 = ((qp >> 8) & 255) - 128, Q2 = ((qp >> 16) & 255) - 128;
+        sh.c.x[s] = xj.x + (R0 * Q0 + R3 * Q1 + R6 * Q2);
+        sh.c.y[s] = xj.y + (R1 * Q0 + R4 * Q1 + R7 * Q2);
+        sh.c.z[s] = xj.z + (R2 * Q0 + R5 * Q1 + R8 * Q2);
+        sh.c.jt[s] = j | ((int)xj.w << 28);
+    }
+}
+
+// Tests atom i against shared slots [0, kp) (kp a multiple of 64, two batches
+// of 32 in flight), appending accepted candidates to out[count..cap) in slot
+// order; returns the new count.
+__device__ __forceinline__ int test_candidates(const NeighShared &sh, int kp, int lane, int i, double xi0, double xi1,
+                                               double xi2, double rc2, int count, int cap, float4 *__restrict__ out)
+{
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t i = blockIdx.x * (int64_t)WARPS + warp; i < N; i += (int64_t)gridDim.x * WARPS) {
-        const StructGrid &g = grid[atom_struct[i]];
-        const double xi0 = xw[3 * i], xi1 = xw[3 * i + 1], xi2 = xw[3 * i + 2];
-        const int local = atom_cell[i] - g.cell_base;
-        const int c2 = local % g.nc[2], c1 = (local / g.nc[2]) % g.nc[1], c0 = local / (g.nc[1] * g.nc[2]);
-        const int w0 = 2 * g.m[0] + 1, w1 = 2 * g.m[1] + 1, w2 = 2 * g.m[2] + 1;
-        const int O = w0 * w1 * w2;
-        int count = 0;
-        for (int ob = 0; ob < O; ob += 32) {
-            const int o = ob + lane;
-            int cnt = 0, start = 0, q0 = 0, q1 = 0, q2 = 0;
-            if (o < O) {
-                const int d2 = o % w2 - g.m[2];
-                const int t = o / w2;
-                const int d1 = t % w1 - g.m[1];
-                const int d0 = t / w1 - g.m[0];
-                const int t0 = c0 + d0, t1 = c1 + d1, t2 = c2 + d2;
-                q0 = floor_div(t0, g.nc[0]);
-                q1 = floor_div(t1, g.nc[1]);
-                q2 = floor_div(t2, g.nc[2]);
-                const int cw = g.cell_base + ((t0 - q0 * g.nc[0]) * g.nc[1] + (t1 - q1 * g.nc[1])) * g.nc[2] + (t2 - q2 * g.nc[2]);
-                cnt = cell_cnt[cw];
-                start = cell_start[cw];
-            }
-            int inc = cnt;
+    for (int kb = 0; kb < kp; kb += 64) {
+        const int ka = kb + lane, kc = ka + 32;
+        const double ax = xi0 - sh.c.x[ka], ay = xi1 - sh.c.y[ka], az = xi2 - sh.c.z[ka];
+        const double cx = xi0 - sh.c.x[kc], cy = xi1 - sh.c.y[kc], cz = xi2 - sh.c.z[kc];
+        const double ra = ax * ax + ay * ay + az * az, rb = cx * cx + cy * cy + cz * cz;
+        bool acca = ra < rc2, accb = rb < rc2;
+        if (acca && !(ra > 1e-12)) acca = (sh.c.jt[ka] & 0x0fffffff) != i;
+        if (accb && !(rb > 1e-12)) accb = (sh.c.jt[kc] & 0x0fffffff) != i;
+        const unsigned ba = __ballot_sync(FULL, acca), bb = __ballot_sync(FULL, accb);
+        if (acca) {
+            const int p = count + __popc(ba & lt);
+            if (p < cap) out[p] = make_float4((float)ax, (float)ay, (float)az, __int_as_float(sh.c.jt[ka]));
+        }
+        count += __popc(ba);
+        if (accb) {
+            const int p = count + __popc(bb & lt);
+            if (p < cap) out[p] = make_float4((float)cx, (float)cy, (float)cz, __int_as_float(sh.c.jt[kc]));
+        }
+        count += __popc(bb);
+    }
+    return count;
+}
+
+__device__ __forceinline__ void finish_atom(int64_t i, int count, int cap, int *__restrict__ nbr_cnt, DevErr *err)
+{
+    nbr_cnt[i] = min(count, cap);
+    if (count > cap) atomicMax(&err->need_cap, count);
+}
+
+// Global-memory search of one atom: lanes take 32 neighbouring cells at a
+// time and then their members, located by a binary search over the lanes'
+// running counts; accepted neighbours are staged in candidate order and then
+// written grouped by type.
+__device__ void search_atom_global(NeighShared &sh, int warp, int lane, int64_t i, const StructGrid &g, int c0, int c1,
+                                   int c2, double xi0, double xi1, double xi2, const double4 *__restrict__ cell_pos,
+                                   const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
+                                   const int *__restrict__ cell_atoms, double rc2, int cap, int ntypes,
+                                   float4 *__restrict__ nbr, int *__restrict__ nbr_cnt, DevErr *err)
+{
+    const unsigned lt = (1u << lane) - 1u;
+    const int O = (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1);
+    int count = 0;
+    for (int ob = 0; ob < O; ob += 32) {
+        const int o = ob + lane;
+        int cnt = 0, start = 0, q0 = 0, q1 = 0, q2 = 0;
+        if (o < O) {
+            const int cw = cell_offset(g, c0, c1, c2, o, q0, q1, q2);
+            cnt = cell_cnt[cw];
+            start = cell_start[cw];
+        }
+        int inc = cnt;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int v = __shfl_up_sync(FULL, inc, d);
-                if (lane >= d) inc += v;
-            }
-            const int exc = inc - cnt;
-            const int total = __shfl_sync(FULL, inc, 31);
-            for (int kb = 0; kb < total; kb += 32) {
-                const int k = kb + lane;
-                int lo = 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(FULL, inc, d);
+            if (lane >= d) inc += v;
+        }
+        const int exc = inc - cnt;
+        const int total = __shfl_sync(FULL, inc, 31);
+        for (int kb = 0; kb < total; kb += 32) {
+            const int k = kb + lane;
+            int lo = 0;
 #pragma unroll
-                for (int step = 16; step; step >>= 1) {
-                    const int ex = __shfl_sync(FULL, exc, lo + step);
-                    if (ex <= k) lo += step;
+            for (int step = 16; step; step >>= 1) {
+                const int ex = __shfl_sync(FULL, exc, lo + step);
+                if (ex <= k) lo += step;
+            }
+            const int st = __shfl_sync(FULL, start, lo);
+            const int ex = __shfl_sync(FULL, exc, lo);
+            const double Q0 = __shfl_sync(FULL, q0, lo), Q1 = __shfl_sync(FULL, q1, lo), Q2 = __shfl_sync(FULL, q2, lo);
+            bool acc = false;
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < total) {
+                const int slot = st + k - ex;
+                const int j = cell_atoms[slot];
+                const double4 xj = cell_pos[slot];
+                const double dx = xi0 - (xj.x + (g.R[0] * Q0 + g.R[3] * Q1 + g.R[6] * Q2));
+                const double dy = xi1 - (xj.y + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
+                const double dz = xi2 - (xj.z + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12)) {
+                    acc = true;
+                    e = make_float4((float)dx, (float)dy, (float)dz, __int_as_float(j | ((int)xj.w << 28)));
                 }
-                const int st = __shfl_sync(FULL, start, lo);
-                const int ex = __shfl_sync(FULL, exc, lo);
-                const double Q0 = __shfl_sync(FULL, q0, lo), Q1 = __shfl_sync(FULL, q1, lo), Q2 = __shfl_sync(FULL, q2, lo);
-                bool acc = false;
-                float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-                int j = 0, tj = 0;
-                if (k < total) {
-                    const int slot = st + k - ex;
-                    j = cell_atoms[slot];
-                    const double4 xj = cell_pos[slot];
-                    const double dx = xi0 - (xj.x + (g.R[0] * Q0 + g.R[3] * Q1 + g.R[6] * Q2));
-                    const double dy = xi1 - (xj.y + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
-                    const double dz = xi2 - (xj.z + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12)) {
-                        acc = true;
-                        e = make_float4((float)dx, (float)dy, (float)dz, 0.f);
-                        tj = (int)xj.w;
+            }
+            const unsigned bal = __ballot_sync(FULL, acc);
+            const int p = count + __popc(bal & lt);
+            if (acc && p < NNP_MAX_NBR) sh.lst[warp][p] = e;
+            count += __popc(bal);
+        }
+    }
+    __syncwarp();
+    const int nw = min(count, NNP_MAX_NBR);
+    int outp = 0;
+    for (int t = 0; t < ntypes; ++t) {
+        for (int kb = 0; kb < nw; kb += 32) {
+            const int k = kb + lane;
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            bool m = false;
+            if (k < nw) {
+                e = sh.lst[warp][k];
+                m = ((unsigned)__float_as_int(e.w) >> 28) == (unsigned)t;
+            }
+            const unsigned bal = __ballot_sync(FULL, m);
+            const int p = outp + __popc(bal & lt);
+            if (m && p < cap) nbr[i * cap + p] = e;
+            outp += __popc(bal);
+        }
+    }
+    if (lane == 0) finish_atom(i, count, cap, nbr_cnt, err);
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(NEIGH_THREADS, 4) k_neigh(int S, const int *__restrict__ ncells,
+                                                          const int *__restrict__ atom_struct,
+                                                          const StructGrid *__restrict__ grid,
+                                                          const double4 *__restrict__ cell_pos,
+                                                          const int *__restrict__ cell_cnt,
+                                                          const int *__restrict__ cell_start,
+                                                          const int *__restrict__ cell_tcnt,
+                                                          const int *__restrict__ cell_atoms, double rc2, int cap,
+                                                          int ntypes, float4 *__restrict__ nbr,
+                                                          int *__restrict__ nbr_cnt, DevErr *err)
+{
+    extern __shared__ __align__(16) unsigned char neigh_smem[];
+    NeighShared &sh = *reinterpret_cast<NeighShared *>(neigh_smem);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int total_cells = grid[S - 1].cell_base + ncells[S - 1];
+    for (int c = blockIdx.x; c < total_cells; c += gridDim.x) {
+        const int na = cell_cnt[c];
+        if (na == 0) continue;                                   // uniform over the block
+        const int cs = cell_start[c];
+        const StructGrid &g = grid[atom_struct[cell_atoms[cs]]];
+        const int local = c - g.cell_base;
+        const int c2 = local % g.nc[2], c1 = (local / g.nc[2]) % g.nc[1], c0 = local / (g.nc[1] * g.nc[2]);
+        const int O = (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1);
+        const int NE = ntypes * O;
+        if (NE > NEIGH_ENT) {
+            for (int a = warp; a < na; a += NNP_WARPS) {
+                const double4 xi = cell_pos[cs + a];
+                search_atom_global(sh, warp, lane, cell_atoms[cs + a], g, c0, c1, c2, xi.x, xi.y, xi.z, cell_pos,
+                                   cell_cnt, cell_start, cell_atoms, rc2, cap, ntypes, nbr, nbr_cnt, err);
+            }
+            __syncthreads();
+            continue;
+        }
+        // segments (type t, neighbouring cell o), type-major
+        for (int e = tid; e < NE; e += NEIGH_THREADS) {
+            const int t = e / O, o = e - t * O;
+            int q0, q1, q2;
+            const int cw = cell_offset(g, c0, c1, c2, o, q0, q1, q2);
+            const int *tc = cell_tcnt + (size_t)cw * ntypes;
+            int s0 = cell_start[cw];
+            for (int u = 0; u < t; ++u) s0 += tc[u];
+            sh.pre[e + 1] = tc[t];
+            sh.start[e] = s0;
+            sh.q[e] = pack_q(q0, q1, q2);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            int run = 0;
+            for (int eb = 0; eb < NE; eb += 32) {
+                const int e = eb + lane;
+                const int v = e < NE ? sh.pre[e + 1] : 0;
+                int inc = v;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int u = __shfl_up_sync(FULL, inc, d);
+                    if (lane >= d) inc += u;
+                }
+                if (e < NE) sh.pre[e + 1] = run + inc;
+                run += __shfl_sync(FULL, inc, 31);
+            }
+            if (lane == 0) sh.pre[0] = 0;
+        }
+        __syncthreads();
+        const int T = sh.pre[NE];
+        if (T <= NEIGH_CAND) {
+            const int kp = (T + 63) & ~63;
+            load_candidates(sh, 0, T, kp, NE, g, cell_pos, cell_atoms, tid);
+            __syncthreads();
+            for (int a = warp; a < na; a += NNP_WARPS) {
+                const int i = cell_atoms[cs + a];
+                const double4 xi = cell_pos[cs + a];
+                const int count = test_candidates(sh, kp, lane, i, xi.x, xi.y, xi.z, rc2, 0, cap, nbr + (int64_t)i * cap);
+                if (lane == 0) finish_atom(i, count, cap, nbr_cnt, err);
+            }
+        } else {
+            for (int a0 = 0; a0 < na; a0 += NEIGH_ATOMS) {
+                const int a1 = min(na, a0 + NEIGH_ATOMS);
+                for (int a = a0 + tid; a < a1; a += NEIGH_THREADS) sh.count[a - a0] = 0;
+                for (int k0 = 0; k0 < T; k0 += NEIGH_CAND) {
+                    const int k1 = min(T, k0 + NEIGH_CAND), kp = (k1 - k0 + 63) & ~63;
+                    __syncthreads();                             // the previous chunk is tested
+                    load_candidates(sh, k0, k1, kp, NE, g, cell_pos, cell_atoms, tid);
+                    __syncthreads();
+                    for (int a = a0 + warp; a < a1; a += NNP_WARPS) {
+                        const int i = cell_atoms[cs + a];
+                        const double4 xi = cell_pos[cs + a];
+                        const int count = test_candidates(sh, kp, lane, i, xi.x, xi.y, xi.z, rc2, sh.count[a - a0],
+                                                          cap, nbr + (int64_t)i * cap);
+                        __syncwarp();
+                        if (lane == 0) sh.count[a - a0] = count;
                     }
                 }
-                const unsigned bal = __ballot_sync(FULL, acc);
-                const int p = count + __popc(bal & lt);
-                if (acc && p < NNP_MAX_NBR) {
-                    s_lst[warp][p] = e;
-                    s_j[warp][p] = j;
-                    s_t[warp][p] = (unsigned char)tj;
-                }
-                count += __popc(bal);
+                __syncthreads();
+                for (int a = a0 + tid; a < a1; a += NEIGH_THREADS) finish_atom(cell_atoms[cs + a], sh.count[a - a0], cap, nbr_cnt, err);
             }
         }
-        __syncwarp();
-        const int nw = min(count, NNP_MAX_NBR);
-        if (count > cap && lane == 0) atomicMax(&err->need_cap, count);
-        int outp = 0;
-        for (int t = 0; t < ntypes; ++t) {
-            for (int kb = 0; kb < nw; kb += 32) {
-                const int k = kb + lane;
-                const bool m = (k < nw) && s_t[warp][k] == t;
-                const unsigned bal = __ballot_sync(FULL, m);
-                const int p = outp + __popc(bal & lt);
-                if (m && p < cap) {
-                    float4 e = s_lst[warp][k];
-                    e.w = __int_as_float(s_j[warp][k] | (t << 28));
-                    nbr[i * cap + p] = e;
-                }
-                outp += __popc(bal);
-            }
-        }
-        if (lane == 0) nbr_cnt[i] = min(count, cap);
-        __syncwarp();
+        __syncthreads();                                         // the shared lists are reused by the next cell
     }
 }
 
@@ -598,6 +804,7 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.cell_cnt.reserve(cell_bound));
     r(E.cell_start.reserve(cell_bound));
     r(E.cell_fill.reserve(cell_bound));
+    r(E.cell_tcnt.reserve(cell_bound * (size_t)std::max(E.dpot.ntypes, 1)));
     r(E.cell_atoms.reserve(N));
     r(E.cell_pos.reserve(N));
     r(E.order.reserve(N));
@@ -638,12 +845,15 @@ std::string run_neighbors(Engine &E, int pbc)
                                                      E.cell_cnt.p);
     k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
-    k_sort_cells<<<S, 128, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p);
+    k_sort_cells<<<S, 128, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes,
+                                    E.cell_atoms.p, E.cell_tcnt.p);
     k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
-    k_neigh<<<grid_for(N, WARPS, num_sms() * 8), WARPS * 32, 0, st>>>(
-        N, E.atom_struct.p, E.atom_cell.p, E.grid.p, E.xw.p, E.cell_pos.p, E.cell_cnt.p, E.cell_start.p, E.cell_atoms.p,
-        rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
+    const int nsm = sizeof(NeighShared);
+    cudaFuncSetAttribute(k_neigh, cudaFuncAttributeMaxDynamicSharedMemorySize, nsm);
+    k_neigh<<<num_sms() * 4, NEIGH_THREADS, nsm, st>>>(S, E.scan_tmp.p, E.atom_struct.p, E.grid.p, E.cell_pos.p,
+                                                       E.cell_cnt.p, E.cell_start.p, E.cell_tcnt.p, E.cell_atoms.p,
+                                                       rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
     E.mark(1);
     return cuda_msg("neighbour list");
 }
