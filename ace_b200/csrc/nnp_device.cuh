@@ -23,7 +23,10 @@
 
 #define NNP_WARPS 8           // warps per block of the per-atom kernels
 #define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
-#define NNP_PCH 192           // pairs per chunk of the force kernel's pair pass
+#define NNP_PCH 256           // pair coefficients the force kernel stores per chunk
+#ifndef NNP_FORCE_CHUNK
+#define NNP_FORCE_CHUNK NNP_PCH   // pairs per chunk of the force kernel (<= NNP_PCH)
+#endif
 #define NNP_FULL 0xffffffffu
 
 #ifdef __CUDACC__
@@ -457,7 +460,7 @@ struct NbrView {
 NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
 {
     return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 2 * ndamp * C +
-           (force ? 4 * C + 3 * C + gstride + 4 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+           (force ? 4 * C + 3 * C + gstride + 3 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
 __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
@@ -482,7 +485,7 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
         v.gy = p; p += C;
         v.gz = p; p += C;
         v.vec = p; p += gstride;
-        v.pc = p; p += 4 * NNP_PCH;
+        v.pc = p; p += 3 * NNP_PCH;
     } else {
         v.gx = v.gy = v.gz = v.vec = v.pc = nullptr;
     }
@@ -587,18 +590,15 @@ __device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
 //    n*floor((n-1)/2) + (n even ? n/2 : 0) = n(n-1)/2 pairs.
 // Lanes step p by 32, which is (q32, r32) = (32/m, 32%m) in (g, f): two
 // adds and one wrap per step instead of a division or a square root.
-// The force kernel stores per-pair coefficients chunk by chunk: a J == K chunk
-// is NNP_PCH consecutive pairs (coefficient index p - c0); a J != K chunk is
-// whole rows a with row stride ps = nb (an odd padded stride, tried to avoid
-// bank conflicts between row owners, measured 2 % slower).
+// The force kernel stores per-pair coefficients chunk by chunk: a chunk is
+// NNP_FORCE_CHUNK consecutive pairs, pair p at coefficient index p - c0
+// (J != K rows may be split between chunks).
 struct Blk {
     int sa, na;       // first member: segment start / size
     int sb, nb;       // second member (sb == sa for J == K)
     bool tri;
     int npairs;
     int m, q32, r32;
-    int ps;           // coefficient row stride (J != K), see above
-    int chunk;        // pairs per force-kernel chunk
 };
 
 __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
@@ -613,8 +613,6 @@ __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
     k.m = k.nb;
     k.q32 = 32 / k.m;
     k.r32 = 32 - k.q32 * k.m;
-    k.ps = k.nb;                                         // nb < NNP_MAX_NBR <= NNP_PCH
-    k.chunk = k.tri ? NNP_PCH : (NNP_PCH / k.ps) * k.nb;
     return true;
 }
 
@@ -651,13 +649,6 @@ __device__ __forceinline__ void pit_slots(const Blk &k, const PairIt &it, int &a
         a = k.sa + it.g;
         b = k.sb + it.f;
     }
-}
-
-// coefficient index of the pair (p, it) in the force chunk that starts at pair
-// c0; row0 = c0 / nb is the chunk's first row (J != K chunks are whole rows)
-__device__ __forceinline__ int pc_index(const Blk &k, const PairIt &it, int p, int c0, int row0)
-{
-    return k.tri ? p - c0 : (it.g - row0) * k.ps + it.f;
 }
 
 // ---------------------------------------------------------------- generic block code
@@ -731,15 +722,14 @@ __device__ void symm_block_generic(const NbrView &v, const DevBlockA &B, const B
     }
 }
 
-// Writes the four dE/dd coefficients of one pair (see force_body); ira, irb
+// Writes the three dE/dd coefficients of one pair (see force_body); ira, irb
 // are the inverse distances.
 __device__ __forceinline__ void pair_coeffs(float *pc, int q, float hc, float hra, float hrb, float cs, float ira,
                                             float irb)
 {
     pc[q] = hra - hc * cs * ira;                 // on u_a in dE/dd_a
-    pc[NNP_PCH + q] = hc * ira;                  // on u_b in dE/dd_a
+    pc[NNP_PCH + q] = hc;                        // on u_b / r_a in dE/dd_a, on u_a / r_b in dE/dd_b
     pc[2 * NNP_PCH + q] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
-    pc[3 * NNP_PCH + q] = hc * irb;              // on u_a in dE/dd_b
 }
 
 // Pair pass of the force kernel for pairs [c0,c1) of one block (any form):
@@ -749,7 +739,6 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
 {
     const float *eb = v.vec + B.off_g;
     const bool gauss = (B.form == ANG_GAUSS);
-    const int row0 = k.tri ? 0 : c0 / k.nb;
     PairIt it = pit_init(k, c0 + lane);
 #pragma unroll 1
     for (int p = c0 + lane; p < c1; p += 32, pit_next(k, it)) {
@@ -802,7 +791,7 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 hrb = fmaf(ef, drb, hrb);
             }
         }
-        pair_coeffs(v.pc, pc_index(k, it, p, c0, row0), hc, hra, hrb, cs, ua.w, ub.w);
+        pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);
     }
 }
 
@@ -814,7 +803,7 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
 // for even n (first member if x < n/2, second member otherwise).
 __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c1, int lane)
 {
-    const float *cA = v.pc, *cB = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH, *cD = v.pc + 3 * NNP_PCH;
+    const float *cA = v.pc, *cH = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH;
     if (k.tri) {
         const int n = k.m, h = (n - 1) >> 1;
         const int gmin = c0 / n, gmax = min((c1 - 1) / n, (n >> 1) - 1);   // rows g = s-1 touching the chunk
@@ -822,6 +811,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
             const int slot = k.sa + x;
             const float4 us = v.u[slot];
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+#pragma unroll 2
             for (int g = gmin; g <= gmax; ++g) {
                 const bool last = (g == h);                  // even n: half row
                 // first member: partner x+g+1
@@ -832,7 +822,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
                         b = (b >= n) ? b - n : b;
                         const float4 ub = v.u[k.sa + b];
                         sa_ += cA[p - c0];
-                        const float bt = cB[p - c0];
+                        const float bt = cH[p - c0];
                         vx = fmaf(bt, ub.x, vx);
                         vy = fmaf(bt, ub.y, vy);
                         vz = fmaf(bt, ub.z, vz);
@@ -846,49 +836,54 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
                     if (p >= c0 && p < c1) {
                         const float4 ua = v.u[k.sa + y];
                         sa_ += cC[p - c0];
-                        const float dt = cD[p - c0];
+                        const float dt = cH[p - c0];
                         vx = fmaf(dt, ua.x, vx);
                         vy = fmaf(dt, ua.y, vy);
                         vz = fmaf(dt, ua.z, vz);
                     }
                 }
             }
-            v.gx[slot] += fmaf(sa_, us.x, vx);
-            v.gy[slot] += fmaf(sa_, us.y, vy);
-            v.gz[slot] += fmaf(sa_, us.z, vz);
+            v.gx[slot] += fmaf(sa_, us.x, us.w * vx);
+            v.gy[slot] += fmaf(sa_, us.y, us.w * vy);
+            v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
         }
         return;
     }
-    // J != K: the chunk is rows [row0, row1), coefficient of (a, b) at
-    // (a - row0) * ps + b.  Row owners read with the odd stride ps across
-    // lanes (distinct banks), column owners consecutively.
-    // Row and column owners run the same loop (no divergent branches): slot
-    // sl walks its j-th pair with coefficient stride qs and partner stride us_.
-    const int row0 = c0 / k.nb, row1 = row0 + (c1 - c0) / k.nb;
+    // J != K: pair p = g * nb + f couples first member sa + g with second
+    // member sb + f.  A row owner reads the run of its row inside the chunk
+    // (stride 1), a column owner one entry per row (stride nb; row owners
+    // read with stride nb across lanes, column owners consecutively).  Row and
+    // column owners run the same loop (no divergent branches): slot sl walks
+    // its j-th pair with coefficient stride qs.
     const int nslots = k.na + k.nb;
     for (int sl = lane; sl < nslots; sl += 32) {
         const bool is_row = sl < k.na;                 // first member of its pairs
         const int slot = is_row ? k.sa + sl : k.sb + (sl - k.na);
         const float4 us = v.u[slot];
         float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        const bool in_rows = sl >= row0 && sl < row1;
-        const int cnt = is_row ? (in_rows ? k.nb : 0) : row1 - row0;
-        const int q0 = is_row ? (sl - row0) * k.ps : sl - k.na;
-        const int qs = is_row ? 1 : k.ps;
-        const float *c1p = is_row ? cA : cC, *c2p = is_row ? cB : cD;
-        const float4 *up = v.u + (is_row ? k.sb : k.sa + row0);
+        // row g = sl: pairs [max(c0, g nb), min(c1, (g+1) nb))
+        const int pb = sl * k.nb, lo = max(c0, pb), hi = min(c1, pb + k.nb);
+        // column f: rows glo .. ghi-1 with c0 <= g nb + f < c1
+        const int f = sl - k.na;
+        const int glo = c0 > f ? (c0 - f + k.nb - 1) / k.nb : 0, ghi = c1 > f ? (c1 - 1 - f) / k.nb + 1 : 0;
+        const int cnt = is_row ? hi - lo : ghi - glo;
+        const int q0 = is_row ? lo - c0 : glo * k.nb + f - c0;
+        const int qs = is_row ? 1 : k.nb;
+        const float *c1p = is_row ? cA : cC;
+        const float4 *up = v.u + (is_row ? k.sb + (lo - pb) : k.sa + glo);
+#pragma unroll 4
         for (int j = 0; j < cnt; ++j) {
             const int q = q0 + j * qs;
             const float4 uo = up[j];
             sa_ += c1p[q];
-            const float bt = c2p[q];
+            const float bt = cH[q];
             vx = fmaf(bt, uo.x, vx);
             vy = fmaf(bt, uo.y, vy);
             vz = fmaf(bt, uo.z, vz);
         }
-        v.gx[slot] += fmaf(sa_, us.x, vx);
-        v.gy[slot] += fmaf(sa_, us.y, vy);
-        v.gz[slot] += fmaf(sa_, us.z, vz);
+        v.gx[slot] += fmaf(sa_, us.x, us.w * vx);
+        v.gy[slot] += fmaf(sa_, us.y, us.w * vy);
+        v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
     }
 }
 
@@ -997,9 +992,10 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
 // d_j = x_i - x_j - R q.  For a triplet (a,b) with dE/dcos = hc,
 // dE/dr_a = hra, dE/dr_b = hrb:
 //   dE/dd_a = (hra - hc cos/r_a) u_a + (hc/r_a) u_b,  and a <-> b.
-// The pair pass writes these four coefficients per pair into shared memory,
-// then each lane owns neighbour slots and sums their pairs in a fixed order
-// (no atomics).  Finally F_j += g_j and F_i -= sum_j g_j in FP64: the
+// The pair pass writes three coefficients per pair into shared memory
+// (hra - hc cos/r_a, hc, hrb - hc cos/r_b), then each lane owns neighbour slots
+// and sums their pairs in a fixed order (no atomics), scaling the sum of the
+// hc u_partner terms by its own 1/r at the end.  Finally F_j += g_j and F_i -= sum_j g_j in FP64: the
 // Newton-3 scatter of nnp.cpp:443-471.
 template <class Blocks>
 __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *__restrict__ rpar,
@@ -1052,8 +1048,8 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             bool staged = false;
-            for (int c0 = 0; c0 < k.npairs; c0 += k.chunk) {
-                const int c1 = min(k.npairs, c0 + k.chunk);
+            for (int c0 = 0; c0 < k.npairs; c0 += NNP_FORCE_CHUNK) {
+                const int c1 = min(k.npairs, c0 + NNP_FORCE_CHUNK);
                 if (!Blocks::force(v, II, tt, k, c0, c1, cap, lane, v.vec + B.off_g)) {
                     if (!staged) {
                         for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
@@ -1134,7 +1130,7 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
     // the force view's per-neighbour gradient arrays hold the relative
     // displacement dv_k = V_i - V_k, and its pair-coefficient area the rate
-    // of change of the distance, rr_k = u_k . dv_k (cap <= NNP_MAX_NBR <= 4 NNP_PCH)
+    // of change of the distance, rr_k = u_k . dv_k (cap <= NNP_MAX_NBR <= 3 NNP_PCH)
     float *rr = v.pc;
     const DevPot &P = *pot;
     const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;

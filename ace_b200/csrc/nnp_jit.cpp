@@ -180,8 +180,7 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
         os << "            const float e" << f << " = eb[" << f << "];\n";
         os << "            const float q" << f << " = e" << f << " * " << flit(fs[f].zeta * fs[f].lf) << ";\n";
     }
-    os << "            const int row0 = k.tri ? 0 : c0 / k.nb;\n"
-          "            PairIt it = pit_init(k, c0 + lane);\n"
+    os << "            PairIt it = pit_init(k, c0 + lane);\n"
           "#pragma unroll NNP_FORCE_UNROLL\n"
           "            for (int p = c0 + lane; p < c1; p += 32, pit_next(k, it)) {\n";
     std::ostringstream body;
@@ -214,7 +213,7 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
         body << "              hra = fmaf(gsp, da" << d << " * wb" << d << ", hra);\n";
         body << "              hrb = fmaf(gsp, wa" << d << " * db" << d << ", hrb); }\n";
     }
-    body << "            pair_coeffs(v.pc, pc_index(k, it, p, c0, row0), hc, hra, hrb, cs, ua.w, ub.w);\n";
+    body << "            pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);\n";
     os << body.str() << "            }\n            return true;\n        }\n";
     return os.str();
 }
@@ -302,7 +301,8 @@ std::string make_source(const Engine &E)
     // the batched workload: 3 blocks make the symmetry-function kernel 7 %
     // faster (72 -> 69 registers, no spills); the force kernel is fastest
     // unconstrained (127 registers; 80 with 3 blocks, 2 % slower).
-    // NNP_SYMM_MINB / NNP_FORCE_MINB / NNP_FORCE_UNROLL override the defaults.
+    // NNP_SYMM_MINB / NNP_FORCE_MINB / NNP_FORCE_UNROLL override the defaults
+    // (1 .. 4).
     auto knob = [](const char *name, int def) {
         const char *v = std::getenv(name);
         const int b = (v && v[0]) ? std::atoi(v) : def;
@@ -310,6 +310,12 @@ std::string make_source(const Engine &E)
     };
     os << "#define NNP_SYMM_MINB " << knob("NNP_SYMM_MINB", 3) << "\n#define NNP_FORCE_MINB "
        << knob("NNP_FORCE_MINB", 1) << "\n#define NNP_FORCE_UNROLL " << knob("NNP_FORCE_UNROLL", 1) << "\n";
+    // NNP_FORCE_CHUNK (1 .. NNP_PCH): pairs per chunk of the force kernel;
+    // small values split the pair rows between many chunks (used by a test)
+    if (const char *c = std::getenv("NNP_FORCE_CHUNK")) {
+        const int n = std::atoi(c);
+        if (n >= 1 && n <= NNP_PCH) os << "#define NNP_FORCE_CHUNK " << n << "\n";
+    }
     os << "#include \"nnp_device.cuh\"\nnamespace nnp {\nstruct JitBlocks {\n";
     std::vector<std::pair<int, std::string>> sy, fo, ta;
     const int T = E.dpot.ntypes, TT = T * (T + 1) / 2;

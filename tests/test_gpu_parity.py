@@ -193,3 +193,39 @@ def test_full_size_properties(tmp_path):
     nat = np.diff(b.atom_off)
     assert (np.abs(E2 - E) / nat).max() < 1e-5
     assert np.abs(F2 - F).max() < 1e-4
+
+
+def test_dense_long_neighbour_lists(tmp_path):
+    """About 200 neighbours per atom, nearly all of one element: the force
+    kernel's pair coefficients of one (centre, pair) block span several chunks
+    and, for the lone atom of the other element, single rows of the J != K
+    block are longer than a chunk and split between chunks.  The forces sum
+    ~20,000 FP32 pair terms per atom and are ~100x larger than in the other
+    cases; their FP32 rounding error is ~1.6e-5 of the largest force component
+    (measured), and the bound is 3e-5 of it."""
+    b = synth.batch_random(52, [120, 90], 2, density=0.22, dirichlet=False)
+    typ = np.ones_like(b.type)
+    typ[b.atom_off[:-1]] = 0                                  # one atom of element 0 per structure
+    b = synth.Batch(b.atom_off, b.pos, typ.astype(np.int32), b.cell)
+    path = make_pot(tmp_path, 3, b)
+    g_err, e_err, f_err, res = compare(path, b)
+    fmax = np.abs(res[4]).max()
+    print("dense: G rel %.2e  E/atom %.2e eV  F %.2e eV/A (max |F| %.3g)" % (g_err, e_err, f_err, fmax))
+    assert g_err < G_RTOL and e_err < E_ATOL and f_err < 3e-5 * fmax
+
+
+@pytest.mark.parametrize("chunk", [7, 32])
+def test_force_chunks_split_rows(tmp_path, monkeypatch, chunk):
+    """The force kernel's pair coefficients in chunks of 7 or 32 pairs (the
+    default is 192), so that nearly every row of every J != K block is split
+    between chunks: the forces still match the oracle to the FP32 bound and
+    the default chunking to rounding (a pair lost or counted twice at a chunk
+    boundary would move a force by a whole pair term, ~1e-3 eV/A or more)."""
+    b = small_batch(3)
+    path = make_pot(tmp_path, 3, b)
+    _, _, _, (E0, F0, _, _, Fo, _) = compare(path, b)
+    monkeypatch.setenv("NNP_FORCE_CHUNK", str(chunk))
+    g_err, e_err, f_err, (E1, F1, _, _, _, _) = compare(path, b)
+    assert f_err < F_ATOL
+    assert np.abs(F1 - F0).max() < 2e-6
+    np.testing.assert_array_equal(E1, E0)
