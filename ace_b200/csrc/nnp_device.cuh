@@ -795,57 +795,74 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
     }
 }
 
-// Slot pass: each lane owns neighbour slots of the block and sums, in a fixed
-// order, the coefficients of the pairs [c0,c1) that contain them.  With the
-// numbering of Blk, slot x of a J == K block is the first member of the pairs
-// (x, x+s mod n) at p = (s-1)n + x and the second member of the pairs
-// (x-s mod n, x) at p = (s-1)n + (x-s mod n), s = 1..(n-1)/2, plus s = n/2
-// for even n (first member if x < n/2, second member otherwise).
+// Slot pass: each lane owns neighbour slots of the block (for J == K blocks of
+// at most 16 slots, one of the two halves of a slot's pairs) and sums, in a
+// fixed order, the coefficients of the pairs [c0,c1) that contain them.  With the numbering of Blk, slot x of a J == K
+// block is the first member of the pairs (x, x+s mod n) at p = (s-1)n + x and
+// the second member of the pairs (x-s mod n, x) at p = (s-1)n + (x-s mod n),
+// s = 1..(n-1)/2, plus s = n/2 for even n (first member if x < n/2, second
+// member otherwise).
+
+// g += sa u + (1/r) v for the slot with unit vector and 1/r us
+__device__ __forceinline__ void slot_add(const NbrView &v, int slot, float4 us, float sa_, float vx, float vy, float vz)
+{
+    v.gx[slot] += fmaf(sa_, us.x, us.w * vx);
+    v.gy[slot] += fmaf(sa_, us.y, us.w * vy);
+    v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
+}
+
+// J == K: the pair of row g in which slot x is the first (second == false) or
+// the second member, if it lies in the chunk
+__device__ __forceinline__ void tri_half(const NbrView &v, const Blk &k, const float *cS, const float *cH, int n,
+                                         int h, int x, bool second, int g, int c0, int c1, float &sa_, float &vx,
+                                         float &vy, float &vz)
+{
+    const bool on = g != h || (second ? x >= (n >> 1) : x < (n >> 1));   // even n: half row g = n/2-1
+    int o = second ? x - g - 1 : x + g + 1;                              // partner
+    o = (o < 0) ? o + n : (o >= n ? o - n : o);
+    const int p = g * n + (second ? o : x);
+    if (on && p >= c0 && p < c1) {
+        const float4 uo = v.u[k.sa + o];
+        sa_ += cS[p - c0];
+        const float t = cH[p - c0];
+        vx = fmaf(t, uo.x, vx);
+        vy = fmaf(t, uo.y, vy);
+        vz = fmaf(t, uo.z, vz);
+    }
+}
+
 __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c1, int lane)
 {
     const float *cA = v.pc, *cH = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH;
     if (k.tri) {
         const int n = k.m, h = (n - 1) >> 1;
-        const int gmin = c0 / n, gmax = min((c1 - 1) / n, (n >> 1) - 1);   // rows g = s-1 touching the chunk
+        const int gmin = c0 / n, gmax = min((c1 - 1) / n, (n >> 1) - 1);   // rows g touching the chunk
+        if (n <= 16) {
+            // lane x sums slot x's first-member pairs, lane n + x its
+            // second-member pairs; the halves meet by a shuffle
+            const bool second = lane >= n;
+            const int x = second ? lane - n : lane;
+            float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+            if (lane < 2 * n) {
+#pragma unroll 2
+                for (int g = gmin; g <= gmax; ++g)
+                    tri_half(v, k, second ? cC : cA, cH, n, h, x, second, g, c0, c1, sa_, vx, vy, vz);
+            }
+            sa_ += __shfl_down_sync(NNP_FULL, sa_, n);
+            vx += __shfl_down_sync(NNP_FULL, vx, n);
+            vy += __shfl_down_sync(NNP_FULL, vy, n);
+            vz += __shfl_down_sync(NNP_FULL, vz, n);
+            if (lane < n) slot_add(v, k.sa + x, v.u[k.sa + x], sa_, vx, vy, vz);
+            return;
+        }
         for (int x = lane; x < n; x += 32) {
-            const int slot = k.sa + x;
-            const float4 us = v.u[slot];
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
 #pragma unroll 2
             for (int g = gmin; g <= gmax; ++g) {
-                const bool last = (g == h);                  // even n: half row
-                // first member: partner x+g+1
-                if (!last || x < (n >> 1)) {
-                    const int p = g * n + x;
-                    if (p >= c0 && p < c1) {
-                        int b = x + g + 1;
-                        b = (b >= n) ? b - n : b;
-                        const float4 ub = v.u[k.sa + b];
-                        sa_ += cA[p - c0];
-                        const float bt = cH[p - c0];
-                        vx = fmaf(bt, ub.x, vx);
-                        vy = fmaf(bt, ub.y, vy);
-                        vz = fmaf(bt, ub.z, vz);
-                    }
-                }
-                // second member: partner y = x-g-1 (mod n)
-                if (!last || x >= (n >> 1)) {
-                    int y = x - g - 1;
-                    y = (y < 0) ? y + n : y;
-                    const int p = g * n + y;
-                    if (p >= c0 && p < c1) {
-                        const float4 ua = v.u[k.sa + y];
-                        sa_ += cC[p - c0];
-                        const float dt = cH[p - c0];
-                        vx = fmaf(dt, ua.x, vx);
-                        vy = fmaf(dt, ua.y, vy);
-                        vz = fmaf(dt, ua.z, vz);
-                    }
-                }
+                tri_half(v, k, cA, cH, n, h, x, false, g, c0, c1, sa_, vx, vy, vz);
+                tri_half(v, k, cC, cH, n, h, x, true, g, c0, c1, sa_, vx, vy, vz);
             }
-            v.gx[slot] += fmaf(sa_, us.x, us.w * vx);
-            v.gy[slot] += fmaf(sa_, us.y, us.w * vy);
-            v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
+            slot_add(v, k.sa + x, v.u[k.sa + x], sa_, vx, vy, vz);
         }
         return;
     }

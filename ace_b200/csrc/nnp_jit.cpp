@@ -510,6 +510,18 @@ std::string jit_build(Engine &E)
     E.jit_symm = (void *)ks;
     E.jit_force = (void *)kf;
     E.jit_tangent = (void *)kt;
+    if (std::getenv("NNP_JIT_VERBOSE")) {        // registers and local memory of the compiled kernels
+        const char *names[3] = {"k_symm_jit", "k_force_jit", "k_tangent_jit"};
+        const void *fns[3] = {(const void *)ks, (const void *)kf, (const void *)kt};
+        for (int q = 0; q < 3; ++q) {
+            cudaFuncAttributes a;
+            if (cudaFuncGetAttributes(&a, fns[q]) == cudaSuccess)
+                std::fprintf(stderr, "nnp jit: %s %d registers, %zu bytes local memory\n", names[q], a.numRegs,
+                             a.localSizeBytes);
+            else
+                cudaGetLastError();
+        }
+    }
     return "";
 }
 
