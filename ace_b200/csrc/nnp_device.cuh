@@ -573,6 +573,19 @@ __device__ __forceinline__ int stage_prefetched(const NbrView &v, int n, int cap
     return stage_records(v, v.raw, n, cap, P, T, lane);
 }
 
+// Lanes of a radial block of n <= 32 functions: G phases per function (the
+// largest power of two with G n <= 32), lane = f G + ph; a lane sums the
+// neighbours s0 + ph, s0 + ph + G, ... of function f and a shuffle tree over
+// the G phases (consecutive lanes) completes the sum.
+__device__ __forceinline__ void radial_lanes(int n, int lane, int &f, int &ph, int &G)
+{
+    G = 1;
+    while (4 * G * n <= 64) G <<= 1;        // 2 G n <= 32
+    const int lg = __ffs(G) - 1;
+    f = lane >> lg;
+    ph = lane & (G - 1);
+}
+
 __device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
 {
     K = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
@@ -974,16 +987,19 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
             const DevBlockR B = T.br[J];
             if (B.n == 0) continue;
             const int s0 = v.seg[J], s1 = v.seg[J + 1];
-            for (int f = lane; f < B.n; f += 32) {
+            int f, ph, G;
+            radial_lanes(B.n, lane, f, ph, G);
+            Acc acc = 0;
+            if (f < B.n) {
                 const float2 q = rpar[B.par + f];
-                Acc acc = 0;
-                for (int k = s0; k < s1; ++k) {
+                for (int k = s0 + ph; k < s1; k += G) {
                     float val, der;
                     radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
                     acc_add(acc, val, 1.f);
                 }
-                Gi[B.off_g + f] = (float)acc;
             }
+            for (int off = 1; off < G; off <<= 1) acc += __shfl_xor_sync(NNP_FULL, acc, off);
+            if (ph == 0 && f < B.n) Gi[B.off_g + f] = (float)acc;
         }
         const int TT = P.ntypes * (P.ntypes + 1) / 2;
         for (int tt = 0; tt < TT; ++tt) {
@@ -1178,16 +1194,19 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
             const DevBlockR B = T.br[J];
             if (B.n == 0) continue;
             const int s0 = v.seg[J], s1 = v.seg[J + 1];
-            for (int f = lane; f < B.n; f += 32) {
+            int f, ph, G;
+            radial_lanes(B.n, lane, f, ph, G);
+            float acc = 0.f;
+            if (f < B.n) {
                 const float2 q = rpar[B.par + f];
-                float acc = 0.f;
-                for (int k = s0; k < s1; ++k) {
+                for (int k = s0 + ph; k < s1; k += G) {
                     float val, der;
                     radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
                     acc = fmaf(der, rr[k], acc);
                 }
-                Ci[B.off_g + f] = acc;
             }
+            for (int off = 1; off < G; off <<= 1) acc += __shfl_xor_sync(NNP_FULL, acc, off);
+            if (ph == 0 && f < B.n) Ci[B.off_g + f] = acc;
         }
         __syncwarp();
         // angular: dG/deps = dG/dcos dcos + dG/dr_a rr_a + dG/dr_b rr_b with
