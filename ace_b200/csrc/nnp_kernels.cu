@@ -248,34 +248,50 @@ __global__ void k_fill(int64_t N, const int *__restrict__ atom_cell, const int *
     cell_atoms[slot] = (int)i;
 }
 
-// one block per structure: insertion sort of every cell's member list by
-// (type, atom index), so the neighbour order does not depend on the order of
-// the atomic insertions, and the count of each type among the members
-__global__ void k_sort_cells(const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
+// one thread per cell (all structures): insertion sort of the cell's member
+// list by (type, atom index), so the neighbour order does not depend on the
+// order of the atomic insertions, and the count of each type among the
+// members.  Lists of up to 64 members are sorted in a local copy.
+__global__ void k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
                              const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
                              const int *__restrict__ type, int ntypes, int *__restrict__ cell_atoms,
                              int *__restrict__ cell_tcnt)
 {
-    const int s = blockIdx.x;
-    const int base = grid[s].cell_base, nc = ncells[s];
-    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-        int *a = cell_atoms + cell_start[base + k];
-        const int n = cell_cnt[base + k];
-        for (int p = 0; p < n; ++p) a[p] |= type[a[p]] << 28;   // atom indices < 2^28, types < 8
-        for (int p = 1; p < n; ++p) {
-            const int v = a[p];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= grid[S - 1].cell_base + ncells[S - 1]) return;
+    int *a = cell_atoms + cell_start[c];
+    const int n = cell_cnt[c];
+    int *tc = cell_tcnt + (size_t)c * ntypes;
+    if (n <= 64) {
+        int key[64];
+        for (int p = 0; p < n; ++p) {
+            const int v = a[p] | (type[a[p]] << 28);            // atom indices < 2^28, types < 8
             int q = p - 1;
-            while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
-            a[q + 1] = v;
+            while (q >= 0 && key[q] > v) { key[q + 1] = key[q]; --q; }
+            key[q + 1] = v;
         }
-        int *tc = cell_tcnt + (size_t)(base + k) * ntypes;
         int p = 0;
         for (int t = 0; t < ntypes; ++t) {
             int q = p;
-            while (q < n && (a[q] >> 28) == t) a[q++] &= 0x0fffffff;
+            while (q < n && (key[q] >> 28) == t) { a[q] = key[q] & 0x0fffffff; ++q; }
             tc[t] = q - p;
             p = q;
         }
+        return;
+    }
+    for (int p = 0; p < n; ++p) a[p] |= type[a[p]] << 28;
+    for (int p = 1; p < n; ++p) {
+        const int v = a[p];
+        int q = p - 1;
+        while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
+        a[q + 1] = v;
+    }
+    int p = 0;
+    for (int t = 0; t < ntypes; ++t) {
+        int q = p;
+        while (q < n && (a[q] >> 28) == t) a[q++] &= 0x0fffffff;
+        tc[t] = q - p;
+        p = q;
     }
 }
 
@@ -845,8 +861,8 @@ std::string run_neighbors(Engine &E, int pbc)
                                                      E.cell_cnt.p);
     k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
-    k_sort_cells<<<S, 128, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes,
-                                    E.cell_atoms.p, E.cell_tcnt.p);
+    k_sort_cells<<<grid_for((int64_t)cell_bound, 128, 1 << 30), 128, 0, st>>>(
+        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes, E.cell_atoms.p, E.cell_tcnt.p);
     k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     const int nsm = sizeof(NeighShared);
