@@ -43,6 +43,7 @@ struct TcPlan {
     int tile[NNP_MAX_LAYERS];    // bf16 offset of region h: A_h [128 x P_h] forward, D_h [128 x P_{h+1}] backward
     int tbytes;                  // bytes of one copy of all activation regions
     int dfloats;                 // f'(z_h) of every hidden layer, [n][128] FP32
+    int vfloats;                 // inpw, inpb, hidden biases, output-layer weights (FP32, after d)
     int total;                   // bytes of the whole plan incl. the header
 };
 
@@ -63,13 +64,17 @@ __host__ __device__ inline void make_plan(const DevType &T, bool split, TcPlan &
     p.wbytes = w * 2;
     p.tbytes = t * 2;
     p.dfloats = d;
+    int v = 2 * T.nodes[0] + T.nodes[p.L - 1];
+    for (int h = 0; h + 1 < p.L; ++h) v += T.nodes[h + 1];
+    p.vfloats = v;
     const int copies = split ? 2 : 1;
-    p.total = HEADER + copies * (p.wbytes + p.tbytes) + 4 * d;
+    p.total = HEADER + copies * (p.wbytes + p.tbytes) + 4 * (d + v);
 }
 
 struct Smem {
     __nv_bfloat16 *w_hi, *w_lo, *t_hi, *t_lo;
     float *d;
+    float *vec;        // [inpw | inpb | bias of hidden layer 0, 1, ... | W_out[0][n]]
     uint64_t *bar;
     uint32_t *slot;
 };
@@ -85,6 +90,7 @@ __device__ inline Smem carve(unsigned char *base, const TcPlan &p, bool split)
     s.t_hi = reinterpret_cast<__nv_bfloat16 *>(q); q += p.tbytes;
     s.t_lo = split ? reinterpret_cast<__nv_bfloat16 *>(q) : nullptr; q += split ? p.tbytes : 0;
     s.d = reinterpret_cast<float *>(q);
+    s.vec = s.d + p.dfloats;
     return s;
 }
 
@@ -183,6 +189,22 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
     uint32_t phase = 0;
     int staged = -1;
     bool ok = true;
+    // The first 64 values of this thread's G row of the next tile are loaded
+    // into registers while the current tile computes.
+    float4 row[16];
+    auto fetch_row = [&](int gg) {
+        if (gg >= ntiles) return;
+        int Tn = 0;
+        while (gg >= first[Tn + 1]) ++Tn;
+        const int jn = (gg - first[Tn]) * TILE + t;
+        const bool ln = jn < type_count[Tn];
+        const float *Gn = G + (ln ? order[base[Tn] + jn] : 0) * (i64)gstride;
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+            row[q] = (ln && 4 * q + 4 <= gstride) ? *reinterpret_cast<const float4 *>(Gn + 4 * q)
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    fetch_row(blockIdx.x);
     for (int g = blockIdx.x; g < ntiles && ok; g += gridDim.x) {
         int T = 0;
         while (g >= first[T + 1]) ++T;
@@ -217,19 +239,52 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                     }
                 }
             }
+            // per-element vectors, read by every thread in the epilogues
+            {
+                float *vb = s.vec + 2 * nin;
+                for (int q = t; q < nin; q += TILE) {
+                    s.vec[q] = inpw[q];
+                    s.vec[nin + q] = inpb[q];
+                }
+                for (int h = 0; h + 1 < L; ++h) {
+                    const float *bh, *wth;
+                    int ws;
+                    layer_ptrs(net, DT, h, bh, wth, ws);
+                    for (int q = t; q < DT.nodes[h + 1]; q += TILE) vb[q] = bh[q];
+                    vb += DT.nodes[h + 1];
+                }
+                for (int q = t; q < DT.nodes[L - 1]; q += TILE) vb[q] = w_out[q * ws_out];
+            }
             staged = T;
         }
+        const int neuron = DT.neuron;
+        const float cn = DT.c, outw0 = outw[0], eoff = outb[0] + b_out[0] * outw[0];
+        const float *v_inpw = s.vec, *v_inpb = s.vec + nin, *v_wout = s.vec + p.vfloats - DT.nodes[L - 1];
         // ---- this thread's atom
         const int j = (g - first[T]) * TILE + t;
         const bool live = j < type_count[T];
         const i64 i = live ? order[base[T] + j] : 0;
         // A_0 = inpw * (G + inpb), zero padded; the row is read as float4
-        // (gstride is a multiple of 4 and rows start 16-byte aligned), all of
-        // it before any use so the loads are in flight together
+        // (gstride is a multiple of 4 and rows start 16-byte aligned): the
+        // first 64 values prefetched during the previous tile, the rest here
         {
+#pragma unroll
+            for (int k0 = 0; k0 < 64; k0 += 8) {            // from the prefetched registers
+                if (k0 < p.P[0]) {
+                    const float4 lo4 = row[k0 / 4], hi4 = row[k0 / 4 + 1];
+                    const float g8[8] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+                    float v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int k = k0 + q;
+                        v[q] = (live && k < nin) ? v_inpw[k] * (g8[q] + v_inpb[k]) : 0.f;
+                    }
+                    store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[0] + tc::kmaj(t, k0, p.P[0]), v);
+                }
+            }
             const float *Gi = G + i * gstride;
 #pragma unroll 4
-            for (int k0 = 0; k0 < p.P[0]; k0 += 8) {
+            for (int k0 = 64; k0 < p.P[0]; k0 += 8) {
                 float4 lo4 = make_float4(0.f, 0.f, 0.f, 0.f), hi4 = lo4;
                 if (live && k0 + 4 <= gstride) lo4 = *reinterpret_cast<const float4 *>(Gi + k0);
                 if (live && k0 + 8 <= gstride) hi4 = *reinterpret_cast<const float4 *>(Gi + k0 + 4);
@@ -238,11 +293,12 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int k = k0 + q;
-                    v[q] = (live && k < nin) ? inpw[k] * (g[q] + inpb[k]) : 0.f;
+                    v[q] = (live && k < nin) ? v_inpw[k] * (g[q] + v_inpb[k]) : 0.f;
                 }
                 store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[0] + tc::kmaj(t, k0, p.P[0]), v);
             }
         }
+        fetch_row(g + gridDim.x);
         // ---- forward through the hidden layers
         float e = 0.f;
         for (int h = 0; h + 1 < L && ok; ++h) {
@@ -250,39 +306,50 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
             ok = gemm(s, p.tile[h], p.wf[h], p.P[h], Po, SPLIT, tmem, phase);
             if (!ok) break;
             const bool last = (h + 2 == L);
-            const float *bh, *wth;
-            int wsh;
-            layer_ptrs(net, DT, h, bh, wth, wsh);
-            int doff = 0;
-            for (int q = 0; q < h; ++q) doff += TILE * DT.nodes[q + 1];
+            int doff = 0, boff = 2 * nin;
+            for (int q = 0; q < h; ++q) {
+                doff += TILE * DT.nodes[q + 1];
+                boff += DT.nodes[q + 1];
+            }
             float *dh = s.d + doff;
-            for (int c0 = 0; c0 < Po; c0 += 8) {
-                float z[8], out[8];
-                tc::tmem_ld8(tmem + lane_base + c0, z);
-                tc::tmem_wait_ld();
+            const float *bh = s.vec + boff;
+            for (int c0 = 0; c0 < Po; c0 += 32) {
+                uint32_t r[4][8];                        // up to 32 columns in flight
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int n = c0 + q;
-                    out[q] = 0.f;
-                    if (n < no) {
-                        float a, d, d2;
-                        activation(DT.neuron, DT.c, z[q] + bh[n], a, d, d2);
-                        dh[n * TILE + t] = d;
-                        if (last) {
-                            // output layer: e = b + sum_n W[0][n] a_n; D = outw W[0][n] f'(z_n)
-                            const float wo = w_out[n * ws_out];
-                            e = fmaf(wo, a, e);
-                            out[q] = outw[0] * wo * d;
-                        } else {
-                            out[q] = a;
+                for (int u = 0; u < 4; ++u)
+                    if (c0 + 8 * u < Po) tc::tmem_ld8_raw(tmem + lane_base + c0 + 8 * u, r[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (c0 + 8 * u < Po) tc::tmem_wait_tie(r[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int cb = c0 + 8 * u;
+                    if (cb >= Po) break;
+                    float out[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int n = cb + q;
+                        out[q] = 0.f;
+                        if (n < no) {
+                            float a, d, d2;
+                            activation(neuron, cn, __uint_as_float(r[u][q]) + bh[n], a, d, d2);
+                            dh[n * TILE + t] = d;
+                            if (last) {
+                                // output layer: e = b + sum_n W[0][n] a_n; D = outw W[0][n] f'(z_n)
+                                const float wo = v_wout[n];
+                                e = fmaf(wo, a, e);
+                                out[q] = outw0 * wo * d;
+                            } else {
+                                out[q] = a;
+                            }
                         }
                     }
+                    // next layer's input A_{h+1}, or (last hidden layer) the first
+                    // backward operand D_h in region h; both have K = P_{h+1}
+                    store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[last ? h : h + 1] + tc::kmaj(t, cb, Po), out);
                 }
-                // next layer's input A_{h+1}, or (last hidden layer) the first
-                // backward operand D_h in region h; both have K = P_{h+1}
-                store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[last ? h : h + 1] + tc::kmaj(t, c0, Po), out);
             }
-            if (last && live) e_atom[i] = outb[0] + (b_out[0] + e) * outw[0];
+            if (last && live) e_atom[i] = eoff + e * outw0;
         }
         if (!ok) break;
         // ---- backward: D_{h-1} = (D_h W_h) * f'(z_{h-1}), dE/dG = (D_0 W_0) * inpw;
@@ -296,28 +363,53 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                 for (int q = 0; q < h - 1; ++q) doff += TILE * DT.nodes[q + 1];
                 const float *dprev = s.d + doff;
                 const int ni = DT.nodes[h];
-                for (int c0 = 0; c0 < Pi; c0 += 8) {
-                    float z[8], out[8];
-                    tc::tmem_ld8(tmem + lane_base + c0, z);
-                    tc::tmem_wait_ld();
+                for (int c0 = 0; c0 < Pi; c0 += 32) {
+                    uint32_t r[4][8];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int n = c0 + q;
-                        out[q] = (n < ni) ? z[q] * dprev[n * TILE + t] : 0.f;
-                    }
-                    store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[h - 1] + tc::kmaj(t, c0, Pi), out);
-                }
-            } else {
-                float *o = dEdG + i * gstride;
-                for (int c0 = 0; c0 < Pi; c0 += 8) {
-                    float z[8];
-                    tc::tmem_ld8(tmem + lane_base + c0, z);
-                    tc::tmem_wait_ld();
-                    if (live) {
+                    for (int u = 0; u < 4; ++u)
+                        if (c0 + 8 * u < Pi) tc::tmem_ld8_raw(tmem + lane_base + c0 + 8 * u, r[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (c0 + 8 * u < Pi) tc::tmem_wait_tie(r[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int cb = c0 + 8 * u;
+                        if (cb >= Pi) break;
+                        float out[8];
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
-                            const int n = c0 + q;
-                            if (n < gstride) o[n] = (n < nin) ? z[q] * inpw[n] : 0.f;
+                            const int n = cb + q;
+                            out[q] = (n < ni) ? __uint_as_float(r[u][q]) * dprev[n * TILE + t] : 0.f;
+                        }
+                        store8(s.t_hi, SPLIT ? s.t_lo : nullptr, p.tile[h - 1] + tc::kmaj(t, cb, Pi), out);
+                    }
+                }
+            } else {
+                // dE/dG row, written as float4 (gstride is a multiple of 4)
+                float *o = dEdG + i * gstride;
+                for (int c0 = 0; c0 < Pi; c0 += 32) {
+                    uint32_t r[4][8];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (c0 + 8 * u < Pi) tc::tmem_ld8_raw(tmem + lane_base + c0 + 8 * u, r[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (c0 + 8 * u < Pi) tc::tmem_wait_tie(r[u]);
+                    if (live) {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int cb = c0 + 8 * u;
+                            if (cb >= Pi) break;
+                            float w[8];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                const int n = cb + q;
+                                w[q] = (n < nin) ? __uint_as_float(r[u][q]) * v_inpw[n] : 0.f;
+                            }
+                            if (cb + 4 <= gstride)
+                                *reinterpret_cast<float4 *>(o + cb) = make_float4(w[0], w[1], w[2], w[3]);
+                            if (cb + 8 <= gstride)
+                                *reinterpret_cast<float4 *>(o + cb + 4) = make_float4(w[4], w[5], w[6], w[7]);
                         }
                     }
                 }

@@ -126,5 +126,23 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// x8 load whose registers are read only after tmem_wait_tie on them
+__device__ __forceinline__ void tmem_ld8_raw(uint32_t taddr, uint32_t (&r)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+
+// Waits for this thread's outstanding TMEM loads, with the registers of one
+// x8 load as operands, so that no use of them is scheduled before the wait
+__device__ __forceinline__ void tmem_wait_tie(uint32_t (&r)[8])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])
+                 :
+                 : "memory");
+}
+
 }  // namespace tc
 }  // namespace nnp
