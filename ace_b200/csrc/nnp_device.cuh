@@ -955,6 +955,8 @@ struct GenericBlocks {
         return false;
     }
     __device__ static bool tangent(const NbrView &, int, int, const Blk &, int, int, float *) { return false; }
+    // radial term of one neighbour in the force kernel
+    __device__ static bool radial_force(int, int, float, float, float, const float *, float &) { return false; }
 };
 
 // ---------------------------------------------------------------- kernel bodies
@@ -1057,15 +1059,18 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
         __syncwarp();
         // radial: lanes own their neighbour slot (initialises g)
         for (int k = lane; k < n; k += 32) {
-            const DevBlockR B = T.br[v.t[k]];
+            const int tk = v.t[k];
+            const DevBlockR B = T.br[tk];
             const float4 u = v.u[k];
             const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
             float amp = 0.f;
-            for (int f = 0; f < B.n; ++f) {
-                const float2 q = rpar[B.par + f];
-                float val, der;
-                radial_fd(B.form, v.r[k], q.x, q.y, fc, fd, val, der);
-                amp = fmaf(v.vec[B.off_g + f], der, amp);
+            if (!Blocks::radial_force(II, tk, v.r[k], fc, fd, v.vec + B.off_g, amp)) {
+                for (int f = 0; f < B.n; ++f) {
+                    const float2 q = rpar[B.par + f];
+                    float val, der;
+                    radial_fd(B.form, v.r[k], q.x, q.y, fc, fd, val, der);
+                    amp = fmaf(v.vec[B.off_g + f], der, amp);
+                }
             }
             v.gx[k] = amp * u.x;
             v.gy[k] = amp * u.y;

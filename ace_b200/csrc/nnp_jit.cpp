@@ -218,6 +218,24 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
     return os.str();
 }
 
+// Radial term of one neighbour in the force kernel for a GAUSSIAN block:
+// amp = sum_f e_f dG_f/dr with dG_f/dr = exp(-g^2) (-2 eta g fc + fc'),
+// g = eta (r - rs), (rs, eta) as literals; relative to the block's first
+// dE/dG (eb).
+std::string gen_radial_force_body(const Engine &E, const DevBlockR &B)
+{
+    std::ostringstream os;
+    os << "        {\n            float amp = 0.f;\n";
+    for (int f = 0; f < B.n; ++f) {
+        const float2 q = E.rpar_host[B.par + f];
+        os << "            { const float g = " << flit(q.y) << " * (r - " << flit(q.x) << ");\n"
+           << "              amp = fmaf(eb[" << f << "], expf(-g * g) * fmaf(" << flit(-2.f * q.y)
+           << " * g, fc, fcd), amp); }\n";
+    }
+    os << "            out = amp;\n            return true;\n        }\n";
+    return os.str();
+}
+
 // Tangent of one GAUSS block's symmetry functions along the displacement
 // field (see tangent_body): per pair dG_f = zeta lf x^(zeta-1) w_a w_b dcos
 // + x^zeta (w'_a w_b rr_a + w_a w'_b rr_b), relative to the block's first
@@ -317,8 +335,13 @@ std::string make_source(const Engine &E)
         if (n >= 1 && n <= NNP_PCH) os << "#define NNP_FORCE_CHUNK " << n << "\n";
     }
     os << "#include \"nnp_device.cuh\"\nnamespace nnp {\nstruct JitBlocks {\n";
-    std::vector<std::pair<int, std::string>> sy, fo, ta;
+    std::vector<std::pair<int, std::string>> sy, fo, ta, ra;
     const int T = E.dpot.ntypes, TT = T * (T + 1) / 2;
+    for (int II = 0; II < T; ++II)
+        for (int J = 0; J < T; ++J) {
+            const DevBlockR &B = E.dpot.t[II].br[J];
+            if (B.n > 0 && B.form == RAD_GAUSSIAN) ra.emplace_back(II * NNP_MAX_TYPES + J, gen_radial_force_body(E, B));
+        }
     for (int II = 0; II < T; ++II)
         for (int tt = 0; tt < TT; ++tt) {
             const DevBlockA &B = E.dpot.t[II].ba[tt];
@@ -335,6 +358,9 @@ std::string make_source(const Engine &E)
           "                                 int lane, const float *eb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
        << group_cases(fo) << "        default: return false;\n        }\n    }\n";
+    os << "    __device__ static bool radial_force(int II, int t, float r, float fc, float fcd, const float *eb, float &out)\n"
+          "    {\n        switch (II * NNP_MAX_TYPES + t) {\n"
+       << group_cases(ra) << "        default: return false;\n        }\n    }\n";
     os << "    __device__ static bool tangent(const NbrView &v, int II, int tt, const Blk &k, int cap, int lane, float *Cb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
        << group_cases(ta) << "        default: return false;\n        }\n    }\n};\n}  // namespace nnp\n";
