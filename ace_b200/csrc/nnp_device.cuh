@@ -586,12 +586,15 @@ __device__ __forceinline__ void radial_lanes(int n, int lane, int &f, int &ph, i
     ph = lane & (G - 1);
 }
 
-__device__ __forceinline__ void tt_decode(int tt, int &J, int &K)
+// p / m for 0 <= p < 2^22 and 1 <= m <= 1024 without an integer division: the
+// approximate float quotient is within one of the exact one, and the two
+// comparisons correct it.
+__device__ __forceinline__ int small_div(int p, int m)
 {
-    K = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
-    while (K * (K + 1) / 2 > tt) --K;
-    while ((K + 1) * (K + 2) / 2 <= tt) ++K;
-    J = tt - K * (K + 1) / 2;
+    int q = (int)__fdividef((float)p, (float)m);
+    q += ((q + 1) * m <= p) ? 1 : 0;
+    q -= (q * m > p) ? 1 : 0;
+    return q;
 }
 
 // One angular block as seen by a warp: segments of the two neighbour types and
@@ -624,7 +627,7 @@ __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
     k.npairs = k.tri ? k.na * (k.na - 1) / 2 : k.na * k.nb;
     if (k.npairs == 0) return false;
     k.m = k.nb;
-    k.q32 = 32 / k.m;
+    k.q32 = small_div(32, k.m);
     k.r32 = 32 - k.q32 * k.m;
     return true;
 }
@@ -636,7 +639,7 @@ struct PairIt {
 __device__ __forceinline__ PairIt pit_init(const Blk &k, int p)
 {
     PairIt it;
-    it.g = p / k.m;
+    it.g = small_div(p, k.m);
     it.f = p - it.g * k.m;
     return it;
 }
@@ -849,7 +852,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
     const float *cA = v.pc, *cH = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH;
     if (k.tri) {
         const int n = k.m, h = (n - 1) >> 1;
-        const int gmin = c0 / n, gmax = min((c1 - 1) / n, (n >> 1) - 1);   // rows g touching the chunk
+        const int gmin = small_div(c0, n), gmax = min(small_div(c1 - 1, n), (n >> 1) - 1);   // rows g touching the chunk
         if (n <= 16) {
             // lane x sums slot x's first-member pairs, lane n + x its
             // second-member pairs; the halves meet by a shuffle
@@ -895,7 +898,8 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
         const int pb = sl * k.nb, lo = max(c0, pb), hi = min(c1, pb + k.nb);
         // column f: rows glo .. ghi-1 with c0 <= g nb + f < c1
         const int f = sl - k.na;
-        const int glo = c0 > f ? (c0 - f + k.nb - 1) / k.nb : 0, ghi = c1 > f ? (c1 - 1 - f) / k.nb + 1 : 0;
+        const int glo = c0 > f ? small_div(c0 - f + k.nb - 1, k.nb) : 0,
+                  ghi = c1 > f ? small_div(c1 - 1 - f, k.nb) + 1 : 0;
         const int cnt = is_row ? hi - lo : ghi - glo;
         const int q0 = is_row ? lo - c0 : glo * k.nb + f - c0;
         const int qs = is_row ? 1 : k.nb;
@@ -1003,12 +1007,11 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
             for (int off = 1; off < G; off <<= 1) acc += __shfl_xor_sync(NNP_FULL, acc, off);
             if (ph == 0 && f < B.n) Gi[B.off_g + f] = (float)acc;
         }
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
+        // angular blocks tt = K (K + 1) / 2 + J, J <= K
+        for (int K = 0, tt = 0; K < P.ntypes; ++K)
+        for (int J = 0; J <= K; ++J, ++tt) {
             const DevBlockA B = T.ba[tt];
             if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             if (!Blocks::template symm<Acc>(v, II, tt, k, cap, lane, Gi + B.off_g)) {
@@ -1077,12 +1080,11 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             v.gz[k] = amp * u.z;
         }
         __syncwarp();
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
+        // angular blocks tt = K (K + 1) / 2 + J, J <= K
+        for (int K = 0, tt = 0; K < P.ntypes; ++K)
+        for (int J = 0; J <= K; ++J, ++tt) {
             const DevBlockA B = T.ba[tt];
             if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             bool staged = false;
@@ -1216,12 +1218,11 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
         __syncwarp();
         // angular: dG/deps = dG/dcos dcos + dG/dr_a rr_a + dG/dr_b rr_b with
         // dcos = (u_b . dv_a - cos rr_a)/r_a + (u_a . dv_b - cos rr_b)/r_b
-        const int TT = P.ntypes * (P.ntypes + 1) / 2;
-        for (int tt = 0; tt < TT; ++tt) {
+        // angular blocks tt = K (K + 1) / 2 + J, J <= K
+        for (int K = 0, tt = 0; K < P.ntypes; ++K)
+        for (int J = 0; J <= K; ++J, ++tt) {
             const DevBlockA B = T.ba[tt];
             if (B.n == 0) continue;
-            int J, K;
-            tt_decode(tt, J, K);
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             if (Blocks::tangent(v, II, tt, k, cap, lane, Ci + B.off_g)) {

@@ -319,8 +319,10 @@ __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const 
 // buffer stream through it in chunks; a cell with more (type, cell) segments
 // than the segment table holds is searched from global memory, one warp per
 // atom, with the same order and arithmetic.
-#define NEIGH_THREADS (NNP_WARPS * 32)
-#define NEIGH_CAND 1536       // candidates held in shared memory at a time (multiple of 64)
+#define NEIGH_WARPS 4         // warps per block of the neighbour search
+#define NEIGH_THREADS (NEIGH_WARPS * 32)
+#define NEIGH_BLOCKS 7        // resident blocks per SM (shared memory)
+#define NEIGH_CAND 768       // candidates held in shared memory at a time (multiple of 64)
 #define NEIGH_ENT 512         // (type, neighbouring cell) segments of one cell's candidate list
 #define NEIGH_ATOMS 1024      // atoms of one cell whose counts are kept while chunks stream
 
@@ -330,7 +332,7 @@ struct NeighShared {
             double x[NEIGH_CAND], y[NEIGH_CAND], z[NEIGH_CAND];   // shifted candidate positions
             int jt[NEIGH_CAND];                                  // j | type << 28
         } c;
-        float4 lst[NNP_WARPS][NNP_MAX_NBR];   // global-memory search: accepted, j | type << 28 in .w
+        float4 lst[NEIGH_WARPS][NNP_MAX_NBR]; // global-memory search: accepted, j | type << 28 in .w
     };
     int count[NEIGH_ATOMS];                   // running neighbour counts (chunked lists)
     int pre[NEIGH_ENT + 1];                   // exclusive scan of the segment lengths
@@ -510,7 +512,7 @@ __device__ void search_atom_global(NeighShared &sh, int warp, int lane, int64_t 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(NEIGH_THREADS, 4) k_neigh(int S, const int *__restrict__ ncells,
+__global__ void __launch_bounds__(NEIGH_THREADS, NEIGH_BLOCKS) k_neigh(int S, const int *__restrict__ ncells,
                                                           const int *__restrict__ atom_struct,
                                                           const StructGrid *__restrict__ grid,
                                                           const double4 *__restrict__ cell_pos,
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(NEIGH_THREADS, 4) k_neigh(int S, const int *__
         const int O = (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1);
         const int NE = ntypes * O;
         if (NE > NEIGH_ENT) {
-            for (int a = warp; a < na; a += NNP_WARPS) {
+            for (int a = warp; a < na; a += NEIGH_WARPS) {
                 const double4 xi = cell_pos[cs + a];
                 search_atom_global(sh, warp, lane, cell_atoms[cs + a], g, c0, c1, c2, xi.x, xi.y, xi.z, cell_pos,
                                    cell_cnt, cell_start, cell_atoms, rc2, cap, ntypes, nbr, nbr_cnt, err);
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(NEIGH_THREADS, 4) k_neigh(int S, const int *__
             const int kp = (T + 63) & ~63;
             load_candidates(sh, 0, T, kp, NE, g, cell_pos, cell_atoms, tid);
             __syncthreads();
-            for (int a = warp; a < na; a += NNP_WARPS) {
+            for (int a = warp; a < na; a += NEIGH_WARPS) {
                 const int i = cell_atoms[cs + a];
                 const double4 xi = cell_pos[cs + a];
                 const int count = test_candidates(sh, kp, lane, i, xi.x, xi.y, xi.z, rc2, 0, cap, nbr + (int64_t)i * cap);
@@ -593,7 +595,7 @@ __global__ void __launch_bounds__(NEIGH_THREADS, 4) k_neigh(int S, const int *__
                     __syncthreads();                             // the previous chunk is tested
                     load_candidates(sh, k0, k1, kp, NE, g, cell_pos, cell_atoms, tid);
                     __syncthreads();
-                    for (int a = a0 + warp; a < a1; a += NNP_WARPS) {
+                    for (int a = a0 + warp; a < a1; a += NEIGH_WARPS) {
                         const int i = cell_atoms[cs + a];
                         const double4 xi = cell_pos[cs + a];
                         const int count = test_candidates(sh, kp, lane, i, xi.x, xi.y, xi.z, rc2, sh.count[a - a0],
@@ -867,7 +869,7 @@ std::string run_neighbors(Engine &E, int pbc)
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     const int nsm = sizeof(NeighShared);
     cudaFuncSetAttribute(k_neigh, cudaFuncAttributeMaxDynamicSharedMemorySize, nsm);
-    k_neigh<<<num_sms() * 4, NEIGH_THREADS, nsm, st>>>(S, E.scan_tmp.p, E.atom_struct.p, E.grid.p, E.cell_pos.p,
+    k_neigh<<<num_sms() * NEIGH_BLOCKS, NEIGH_THREADS, nsm, st>>>(S, E.scan_tmp.p, E.atom_struct.p, E.grid.p, E.cell_pos.p,
                                                        E.cell_cnt.p, E.cell_start.p, E.cell_tcnt.p, E.cell_atoms.p,
                                                        rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
     E.mark(1);
