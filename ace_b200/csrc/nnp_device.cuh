@@ -860,7 +860,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
             const int x = second ? lane - n : lane;
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
             if (lane < 2 * n) {
-#pragma unroll 2
+#pragma unroll 1
                 for (int g = gmin; g <= gmax; ++g)
                     tri_half(v, k, second ? cC : cA, cH, n, h, x, second, g, c0, c1, sa_, vx, vy, vz);
             }
@@ -873,7 +873,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
         }
         for (int x = lane; x < n; x += 32) {
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-#pragma unroll 2
+#pragma unroll 1
             for (int g = gmin; g <= gmax; ++g) {
                 tri_half(v, k, cA, cH, n, h, x, false, g, c0, c1, sa_, vx, vy, vz);
                 tri_half(v, k, cC, cH, n, h, x, true, g, c0, c1, sa_, vx, vy, vz);
@@ -905,7 +905,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
         const int qs = is_row ? 1 : k.nb;
         const float *c1p = is_row ? cA : cC;
         const float4 *up = v.u + (is_row ? k.sb + (lo - pb) : k.sa + glo);
-#pragma unroll 4
+#pragma unroll 2
         for (int j = 0; j < cnt; ++j) {
             const int q = q0 + j * qs;
             const float4 uo = up[j];
