@@ -316,9 +316,10 @@ std::string make_source(const Engine &E)
     // Launch-bound and unroll choices, as macros at the top of the source.
     // Resident blocks per SM the compiler budgets registers for (at most 255,
     // 128, 85, 64 registers for 1..4 blocks of NNP_WARPS warps).  Measured on
-    // the batched workload: 3 blocks make the symmetry-function kernel 7 %
-    // faster (72 -> 69 registers, no spills); the force kernel is fastest
-    // unconstrained (127 registers; 80 with 3 blocks, 2 % slower).
+    // the batched workload: 4 blocks make the symmetry-function kernel 3 %
+    // faster than 3 (64 instead of 71 registers; its shared memory allows 4);
+    // the force kernel is fastest unconstrained (115 registers, 2 blocks by
+    // its shared memory; capped at 128 registers it is 3 % slower).
     // NNP_SYMM_MINB / NNP_FORCE_MINB / NNP_FORCE_UNROLL override the defaults
     // (1 .. 4).
     auto knob = [](const char *name, int def) {
@@ -326,7 +327,7 @@ std::string make_source(const Engine &E)
         const int b = (v && v[0]) ? std::atoi(v) : def;
         return (b >= 1 && b <= 4) ? b : def;
     };
-    os << "#define NNP_SYMM_MINB " << knob("NNP_SYMM_MINB", 3) << "\n#define NNP_FORCE_MINB "
+    os << "#define NNP_SYMM_MINB " << knob("NNP_SYMM_MINB", 4) << "\n#define NNP_FORCE_MINB "
        << knob("NNP_FORCE_MINB", 1) << "\n#define NNP_FORCE_UNROLL " << knob("NNP_FORCE_UNROLL", 1) << "\n";
     // NNP_FORCE_CHUNK (1 .. NNP_PCH): pairs per chunk of the force kernel;
     // small values split the pair rows between many chunks (used by a test)
