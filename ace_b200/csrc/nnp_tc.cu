@@ -120,6 +120,26 @@ __device__ __forceinline__ void layer_ptrs(const float *net, const DevType &T, i
     ws = wt_stride(T.nodes[l + 1]);
 }
 
+// Activation and slope in the epilogues: tanh inline, the other forms through
+// one out-of-line copy of the generic switch, so the unrolled epilogue loops
+// stay small (instruction fetch limited the kernel).
+__device__ __noinline__ void activation_call(int neuron, float c, float z, float &a, float &d)
+{
+    float d2;
+    activation(neuron, c, z, a, d, d2);
+}
+
+__device__ __forceinline__ void tc_activation(int neuron, float c, float z, float &a, float &d)
+{
+    if (neuron == NEU_TANH) {
+        const float t = tanhf(c * z);
+        a = t;
+        d = c * (1.f - t * t);
+    } else {
+        activation_call(neuron, c, z, a, d);
+    }
+}
+
 // One MMA chain D[128 x N] = A[128 x K] * B[N x K]^T issued by thread 0 and
 // waited for by every thread.  Returns false when the wait gave up.
 __device__ bool gemm(const Smem &s, int a_off, int b_off, int K, int N, bool split, uint32_t tmem, uint32_t &phase)
@@ -331,8 +351,8 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                         const int n = cb + q;
                         out[q] = 0.f;
                         if (n < no) {
-                            float a, d, d2;
-                            activation(neuron, cn, __uint_as_float(r[u][q]) + bh[n], a, d, d2);
+                            float a, d;
+                            tc_activation(neuron, cn, __uint_as_float(r[u][q]) + bh[n], a, d);
                             dh[n * TILE + t] = d;
                             if (last) {
                                 // output layer: e = b + sum_n W[0][n] a_n; D = outw W[0][n] f'(z_n)
