@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
                 for (int q = t; q < DT.nodes[L - 1]; q += TILE) vb[q] = w_out[q * ws_out];
             }
             staged = T;
+            __syncthreads();        // the vectors are read below by every thread (A_0 conversion)
         }
         const int neuron = DT.neuron;
         const float cn = DT.c, outw0 = outw[0], eoff = outb[0] + b_out[0] * outw[0];

@@ -65,3 +65,32 @@ def test_precision_switch_back_to_fp32(tmp_path):
     E1, F1 = nn.compute_batch(z["atom_off"], z["pos"], z["type"], z["cell"])
     nn.close()
     assert np.abs(E1 - E0).max() < 1e-9 and np.abs(F1 - F0).max() < 1e-7
+
+
+def test_bf16x3_many_tiles_four_elements(tmp_path):
+    """Config-5 potential (4 elements, 64-48-48-1) on 400 structures of its
+    stream (~150 k atoms): the tensor-core kernel's CTAs run several tiles and
+    restage weights and per-element vectors when the element changes.  BF16X3
+    against the FP32 networks on the same handle, every call of three: the
+    BF16X3 rounding is ~5e-5 eV/A on these forces (measured), bounded here by
+    5e-4 eV/A and 5e-5 eV/atom."""
+    from ace_b200 import potential, synth
+    pot = synth.potential_config(5, seed=1234)
+    path = str(tmp_path / "pot5.nnp")
+    potential.write(path, pot)
+    full = synth.config5(n_struct=400)
+    nn = NNP.read(path)
+    _, _, G = nn.compute_batch(full.atom_off[:33] - 0, full.pos[:full.atom_off[32]], full.type[:full.atom_off[32]],
+                               full.cell[:32], symm=True)
+    nn.close()
+    synth.condition(pot, G, full.type[:full.atom_off[32]])
+    potential.write(path, pot)
+    nn = NNP.read(path)
+    E0, F0 = nn.compute_batch(full.atom_off, full.pos, full.type, full.cell)
+    nn.set_precision(2)
+    nat = np.maximum(np.diff(full.atom_off), 1)
+    for _ in range(3):
+        E1, F1 = nn.compute_batch(full.atom_off, full.pos, full.type, full.cell)
+        assert (np.abs(E1 - E0) / nat).max() < 5e-5
+        assert np.abs(F1 - F0).max() < 5e-4
+    nn.close()
