@@ -504,8 +504,17 @@ def add_cpu_baseline(line, name, nn, b, ppath, E_chk, F_chk):
         err_f = max(err_f, float(np.abs(Fs[a0:a1] - f_ref).max()))
     line["cpu_baseline"] = {"value": round(v1, 1), "unit": UNIT, "cores": min(procs, sample.n_struct),
                             "kind": ref_kind(), "sample": "%s, %.1f s wall" % (desc, dt)}
+    # the bound this precision is held to: the FP32 path's parity tolerances,
+    # or 1 meV/atom and 10 meV/A for the tensor-core networks
+    fp32 = line["config"]["network_precision"] == "fp32"
+    e_tol, f_tol = (2e-6, 1e-4) if fp32 else (1e-3, 1e-2)
+    ok = err_e <= e_tol and err_f <= f_tol
     line["error_vs_fp64"] = {"energy_eV_per_atom_max": err_e, "force_eV_per_A_max": err_f, "sample": desc,
-                             "against": ref_kind()}
+                             "against": ref_kind(), "bound": {"energy_eV_per_atom": e_tol, "force_eV_per_A": f_tol},
+                             "within_bound": ok}
+    if not ok:
+        print("bench.py: results differ from the reference beyond the bound (energy %.3g eV/atom, force %.3g eV/A)"
+              % (err_e, err_f), file=sys.stderr)
 
 
 def time_train(args, nn, b, ppath, world, dist, clocks, dev):
