@@ -441,6 +441,11 @@ __device__ __forceinline__ void acc_add(double &acc, float a, float b) { acc += 
 
 // ---------------------------------------------------------------- per-atom staging
 
+// Index of damping group d of neighbour k in NbrView::w / wd: the groups are
+// stored in pairs, (w_2m, w_2m+1) of a neighbour adjacent, so that one 8-byte
+// load reads two groups.
+NNP_HD inline int wix(int d, int k, int cap) { return 2 * ((d >> 1) * cap + k) + (d & 1); }
+
 // Per-warp shared-memory view of one atom's neighbours.
 struct NbrView {
     float4 *u;          // unit vector to the neighbour and inverse distance (ux, uy, uz, 1/r) [C]
@@ -449,7 +454,7 @@ struct NbrView {
     float4 *raw;        // next atom's neighbour records, prefetched (force views) [C]
     int *j;             // neighbour atom index [C]
     float *fc, *fd;     // cutoff value / slope [ncut][C]
-    float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr [ndamp][C]
+    float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr, groups in pairs (wix)
     float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
     float *vec;         // dE/dG row [gstride]
     float *pc;          // pair coefficients [4][NNP_PCH]
@@ -459,7 +464,7 @@ struct NbrView {
 
 NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
 {
-    return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 2 * ndamp * C +
+    return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 4 * ((ndamp + 1) / 2) * C +
            (force ? 4 * C + 3 * C + gstride + 3 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
@@ -478,8 +483,8 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
     v.j = reinterpret_cast<int *>(p); p += C;
     v.fc = p; p += ncut * C;
     v.fd = p; p += ncut * C;
-    v.w = p; p += ndamp * C;
-    v.wd = p; p += ndamp * C;
+    v.w = p; p += 2 * ((ndamp + 1) / 2) * C;                        // 8-byte aligned (C % 8 == 0)
+    v.wd = p; p += 2 * ((ndamp + 1) / 2) * C;
     if (force) {
         v.gx = p; p += C;
         v.gy = p; p += C;
@@ -521,8 +526,8 @@ __device__ __forceinline__ int stage_records(const NbrView &v, const float4 *src
             const float a = T.damp_a[d];
             const float ex = expf(-a * r * r);
             const float f = v.fc[c * cap + k], g = v.fd[c * cap + k];
-            v.w[d * cap + k] = f * ex;
-            v.wd[d * cap + k] = (g - 2.f * a * r * f) * ex;
+            v.w[wix(d, k, cap)] = f * ex;
+            v.wd[wix(d, k, cap)] = (g - 2.f * a * r * f) * ex;
         }
     }
     // type segment starts (the list is grouped by type)
@@ -698,7 +703,7 @@ __device__ void symm_block_generic(const NbrView &v, const DevBlockA &B, const B
                         const int d = pk & 0xff, iz = (pk >> 8) - 1;
                         if (d != dcur) {
                             dcur = d;
-                            damp = v.w[d * cap + a] * v.w[d * cap + b];
+                            damp = v.w[wix(d, a, cap)] * v.w[wix(d, b, cap)];
                         }
                         float pz, pm1;
                         ang_pow(cs, q.x, q.y, iz, pz, pm1);
@@ -772,10 +777,10 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 const int d = pk & 0xff, iz = (pk >> 8) - 1;
                 if (d != dcur) {
                     if (dcur >= 0) {
-                        const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                        const float wa = v.w[wix(dcur, a, cap)], wb = v.w[wix(dcur, b, cap)];
                         hc = fmaf(sc, wa * wb, hc);
-                        hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
-                        hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
+                        hra = fmaf(sp, v.wd[wix(dcur, a, cap)] * wb, hra);
+                        hrb = fmaf(sp, wa * v.wd[wix(dcur, b, cap)], hrb);
                     }
                     dcur = d;
                     sc = 0.f;
@@ -788,10 +793,10 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 sp = fmaf(ef, pz, sp);
             }
             if (dcur >= 0) {
-                const float wa = v.w[dcur * cap + a], wb = v.w[dcur * cap + b];
+                const float wa = v.w[wix(dcur, a, cap)], wb = v.w[wix(dcur, b, cap)];
                 hc = fmaf(sc, wa * wb, hc);
-                hra = fmaf(sp, v.wd[dcur * cap + a] * wb, hra);
-                hrb = fmaf(sp, wa * v.wd[dcur * cap + b], hrb);
+                hra = fmaf(sp, v.wd[wix(dcur, a, cap)] * wb, hra);
+                hrb = fmaf(sp, wa * v.wd[wix(dcur, b, cap)], hrb);
             }
         } else {
             const float ca = v.fc[B.cut * cap + a], cb = v.fc[B.cut * cap + b];

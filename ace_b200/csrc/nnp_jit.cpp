@@ -122,12 +122,22 @@ void pair_prologue(std::ostringstream &os, const std::vector<Fn> &fs, std::vecto
     }
     for (size_t b = 0; b < bases.size(); ++b)
         os << "            const float x" << b << " = fabsf(fmaf(" << flit(bases[b]) << ", cs, 0.5f));\n";
-    for (int d : damps) {
-        os << "            const float wa" << d << " = v.w[" << d << " * cap + a], wb" << d << " = v.w[" << d
-           << " * cap + b];\n";
+    // damping factors: groups 2m and 2m+1 of a neighbour are one float2 (wix)
+    std::set<int> pairs;
+    for (int d : damps) pairs.insert(d >> 1);
+    for (int m : pairs) {
+        const std::string M = std::to_string(m);
+        os << "            const float2 wpa" << M << " = reinterpret_cast<const float2 *>(v.w)[" << M
+           << " * cap + a], wpb" << M << " = reinterpret_cast<const float2 *>(v.w)[" << M << " * cap + b];\n";
         if (force)
-            os << "            const float da" << d << " = v.wd[" << d << " * cap + a], db" << d << " = v.wd[" << d
-               << " * cap + b];\n";
+            os << "            const float2 dpa" << M << " = reinterpret_cast<const float2 *>(v.wd)[" << M
+               << " * cap + a], dpb" << M << " = reinterpret_cast<const float2 *>(v.wd)[" << M << " * cap + b];\n";
+    }
+    for (int d : damps) {
+        const std::string M = std::to_string(d >> 1), c = (d & 1) ? ".y" : ".x";
+        os << "            const float wa" << d << " = wpa" << M << c << ", wb" << d << " = wpb" << M << c << ";\n";
+        if (force)
+            os << "            const float da" << d << " = dpa" << M << c << ", db" << d << " = dpb" << M << c << ";\n";
         else
             os << "            const float w" << d << " = wa" << d << " * wb" << d << ";\n";
     }
