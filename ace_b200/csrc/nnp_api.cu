@@ -646,9 +646,13 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
         N = b->atom_off[S];
         if (N >= (int64_t)1 << 28) return fail(h, NNP_ERR_CAPACITY, "more than 2^28 atoms in one batch");
         const int T = E.host.ntypes();
-        for (int64_t i = 0; i < N; ++i)
-            if (b->type[i] < 0 || b->type[i] >= T)
-                return fail(h, NNP_ERR_TYPE, "atom " + std::to_string(i) + " has type index " + std::to_string(b->type[i]) + " outside [0," + std::to_string(T) + ")");
+        // a branch-free pass (vectorised), then the first bad atom for the message
+        unsigned any_bad = 0;
+        for (int64_t i = 0; i < N; ++i) any_bad |= (unsigned)b->type[i] >= (unsigned)T;
+        if (any_bad)
+            for (int64_t i = 0; i < N; ++i)
+                if (b->type[i] < 0 || b->type[i] >= T)
+                    return fail(h, NNP_ERR_TYPE, "atom " + std::to_string(i) + " has type index " + std::to_string(b->type[i]) + " outside [0," + std::to_string(T) + ")");
         E.cap = std::max(E.cap, estimate_cap(b, E.host.rc));
         // inputs -> device
         const size_t bo = sizeof(int64_t) * (S + 1), bp = sizeof(double) * 3 * N, bt = sizeof(int32_t) * N,
