@@ -457,7 +457,7 @@ struct NbrView {
     float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr, groups in pairs (wix)
     float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
     float *vec;         // dE/dG row [gstride]
-    float *pc;          // pair coefficients [4][NNP_PCH]
+    float *pc;          // pair coefficients [3][NNP_PCH]
     int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
     unsigned char *t;   // neighbour type [C]
 };
