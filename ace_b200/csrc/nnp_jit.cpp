@@ -150,6 +150,46 @@ int base_of(const std::vector<float> &bases, float lf)
     return 0;
 }
 
+// Sums over the warp of the per-lane accumulators s0 .. s(nf-1), stored to
+// dst[f] by one lane each.  The list (padded with zeros to a power of two) is
+// halved at each shuffle offset: a lane keeps one half and adds its partner's
+// copy of that half, so nf values cost about nf shuffles instead of 5 nf; once
+// one value is left the remaining offsets are plain butterflies.  The lane's
+// offset bits then give the index of the sum it holds.
+std::string gen_reduce_store(size_t nf, const std::string &acc, const std::string &dst, bool to_float)
+{
+    std::ostringstream os;
+    size_t p2 = 1;
+    while (p2 < nf) p2 <<= 1;
+    std::vector<std::string> L;
+    for (size_t f = 0; f < p2; ++f) L.push_back(f < nf ? "s" + std::to_string(f) : "(" + acc + ")0");
+    std::string idx = "0";
+    int dup = 0, tmp = 0;
+    for (int o = 16; o >= 1; o >>= 1) {
+        const std::string O = std::to_string(o);
+        if (L.size() == 1) {
+            os << "            " << L[0] << " += __shfl_xor_sync(NNP_FULL, " << L[0] << ", " << O << ");\n";
+            dup |= o;
+            continue;
+        }
+        const size_t h = L.size() / 2;
+        os << "            const bool hb" << O << " = (lane & " << O << ") != 0;\n";
+        std::vector<std::string> N;
+        for (size_t i = 0; i < h; ++i) {
+            const std::string t = "rs" + std::to_string(tmp++);
+            os << "            " << acc << " " << t << " = (hb" << O << " ? " << L[h + i] << " : " << L[i]
+               << ") + __shfl_xor_sync(NNP_FULL, hb" << O << " ? " << L[i] << " : " << L[h + i] << ", " << O << ");\n";
+            N.push_back(t);
+        }
+        idx += " + (hb" + O + " ? " + std::to_string(h) + " : 0)";
+        L = N;
+    }
+    os << "            { const int fi = " << idx << ";\n"
+       << "              if ((lane & " << dup << ") == 0 && fi < " << nf << ") " << dst << "[fi] = "
+       << (to_float ? "(float)" : "") << L[0] << "; }\n";
+    return os.str();
+}
+
 // Body of one GAUSS block's symmetry functions; written relative to the
 // block's first function (Gb), so blocks with equal parameters share it.
 std::string gen_symm_body(const Engine &E, const DevBlockA &B)
@@ -171,10 +211,8 @@ std::string gen_symm_body(const Engine &E, const DevBlockA &B)
         body << "            acc_add(s" << f << ", " << x << ", w" << fs[f].damp << ");\n";
     }
     os << body.str() << "            }\n";
-    for (size_t f = 0; f < fs.size(); ++f) os << "            s" << f << " = warp_sum(s" << f << ");\n";
-    os << "            if (lane == 0) {\n";
-    for (size_t f = 0; f < fs.size(); ++f) os << "                Gb[" << f << "] = (float)s" << f << ";\n";
-    os << "            }\n            return true;\n        }\n";
+    os << gen_reduce_store(fs.size(), "Acc", "Gb", true);
+    os << "            return true;\n        }\n";
     return os.str();
 }
 
@@ -291,10 +329,8 @@ std::string gen_tangent_body(const Engine &E, const DevBlockA &B)
                  << ");\n";
     }
     os << body.str() << "            }\n";
-    for (size_t f = 0; f < fs.size(); ++f) os << "            s" << f << " = warp_sum(s" << f << ");\n";
-    os << "            if (lane == 0) {\n";
-    for (size_t f = 0; f < fs.size(); ++f) os << "                Cb[" << f << "] = s" << f << ";\n";
-    os << "            }\n            return true;\n        }\n";
+    os << gen_reduce_store(fs.size(), "float", "Cb", false);
+    os << "            return true;\n        }\n";
     return os.str();
 }
 
