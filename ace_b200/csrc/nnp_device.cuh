@@ -23,7 +23,7 @@
 
 #define NNP_WARPS 8           // warps per block of the per-atom kernels
 #define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
-#define NNP_PCH 256           // pair coefficients the force kernel stores per chunk
+#define NNP_PCH 288           // pair coefficients the force kernel stores per chunk
 #ifndef NNP_FORCE_CHUNK
 #define NNP_FORCE_CHUNK NNP_PCH   // pairs per chunk of the force kernel (<= NNP_PCH)
 #endif

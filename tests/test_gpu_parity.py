@@ -197,12 +197,13 @@ def test_full_size_properties(tmp_path):
 
 def test_dense_long_neighbour_lists(tmp_path):
     """About 200 neighbours per atom, nearly all of one element: the force
-    kernel's pair coefficients of one (centre, pair) block span several chunks
-    and, for the lone atom of the other element, single rows of the J != K
-    block are longer than a chunk and split between chunks.  The forces sum
-    ~20,000 FP32 pair terms per atom and are ~100x larger than in the other
-    cases; their FP32 rounding error is ~1.6e-5 of the largest force component
-    (measured), and the bound is 3e-5 of it."""
+    kernel's pair coefficients of one (centre, pair) block span several
+    chunks, and the ~200-pair rows of the lone atom's J != K block straddle
+    chunk boundaries (rows longer than a chunk are covered by the forced small
+    chunks of the next test).  The forces sum ~20,000 FP32 pair terms per atom
+    and are ~100x larger than in the other cases; their FP32 rounding error is
+    ~1.6e-5 of the largest force component (measured), and the bound is 3e-5
+    of it."""
     b = synth.batch_random(52, [120, 90], 2, density=0.22, dirichlet=False)
     typ = np.ones_like(b.type)
     typ[b.atom_off[:-1]] = 0                                  # one atom of element 0 per structure
@@ -217,7 +218,7 @@ def test_dense_long_neighbour_lists(tmp_path):
 @pytest.mark.parametrize("chunk", [7, 32])
 def test_force_chunks_split_rows(tmp_path, monkeypatch, chunk):
     """The force kernel's pair coefficients in chunks of 7 or 32 pairs (the
-    default is 192), so that nearly every row of every J != K block is split
+    default is 288), so that nearly every row of every J != K block is split
     between chunks: the forces still match the oracle to the FP32 bound and
     the default chunking to rounding (a pair lost or counted twice at a chunk
     boundary would move a force by a whole pair term, ~1e-3 eV/A or more)."""
