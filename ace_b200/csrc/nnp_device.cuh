@@ -989,6 +989,7 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
     for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
         const i64 i = order[idx];
         const int II = type[i];
+        if ((unsigned)II >= (unsigned)P.ntypes) continue;        // type out of range (reported by the call)
         const DevType &T = P.t[II];
         stage_records(v, nbr + i * cap, nbr_cnt[i], cap, P, T, lane);
         float *Gi = G + i * gstride;
@@ -1059,6 +1060,12 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
     for (i64 idx = idx0; idx < N; idx += stride) {
         const i64 i = i_next;
         const int II = type[i];
+        if ((unsigned)II >= (unsigned)P.ntypes) {               // type out of range (reported by the call)
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncwarp();
+            prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
+            continue;
+        }
         const DevType &T = P.t[II];
         const int n = stage_prefetched(v, n_next, cap, P, T, lane);
         prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
@@ -1185,6 +1192,12 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
     for (i64 idx = idx0; idx < N; idx += stride) {
         const i64 i = i_next;
         const int II = type[i];
+        if ((unsigned)II >= (unsigned)P.ntypes) {               // type out of range (reported by the call)
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncwarp();
+            prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
+            continue;
+        }
         const DevType &T = P.t[II];
         const int n = stage_prefetched(v, n_next, cap, P, T, lane);
         prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);

@@ -68,35 +68,37 @@ __global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N,
 
 // Atoms grouped by element: per-block counts in shared memory, one global
 // atomic per (block, element) to count, then one to reserve each block's range.
+// Atoms whose type is outside [0, ntypes) go last, in slot ntypes (the kernels
+// that walk the order skip them; the call reports the bad type).
 __global__ void k_type_count(int64_t N, const int *__restrict__ type, int ntypes, int *__restrict__ cnt)
 {
-    __shared__ int c[NNP_MAX_TYPES];
-    if (threadIdx.x < NNP_MAX_TYPES) c[threadIdx.x] = 0;
+    __shared__ int c[NNP_MAX_TYPES + 1];
+    if (threadIdx.x <= NNP_MAX_TYPES) c[threadIdx.x] = 0;
     __syncthreads();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < N) {
         const int t = type[i];
-        if (t >= 0 && t < ntypes) atomicAdd(&c[t], 1);
+        atomicAdd(&c[(t >= 0 && t < ntypes) ? t : ntypes], 1);
     }
     __syncthreads();
-    if (threadIdx.x < ntypes && c[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], c[threadIdx.x]);
+    if (threadIdx.x <= ntypes && c[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], c[threadIdx.x]);
 }
 
 __global__ void k_type_scatter(int64_t N, const int *__restrict__ type, int ntypes, const int *__restrict__ cnt,
                                int *__restrict__ fill, int *__restrict__ order)
 {
-    __shared__ int c[NNP_MAX_TYPES], base[NNP_MAX_TYPES];
-    if (threadIdx.x < NNP_MAX_TYPES) c[threadIdx.x] = 0;
+    __shared__ int c[NNP_MAX_TYPES + 1], base[NNP_MAX_TYPES + 1];
+    if (threadIdx.x <= NNP_MAX_TYPES) c[threadIdx.x] = 0;
     __syncthreads();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int t = -1, r = 0;
     if (i < N) {
         t = type[i];
-        if (t >= 0 && t < ntypes) r = atomicAdd(&c[t], 1);
-        else t = -1;
+        if (!(t >= 0 && t < ntypes)) t = ntypes;
+        r = atomicAdd(&c[t], 1);
     }
     __syncthreads();
-    if (threadIdx.x < ntypes) {
+    if (threadIdx.x <= ntypes) {
         int start = 0;
         for (int k = 0; k < (int)threadIdx.x; ++k) start += cnt[k];
         base[threadIdx.x] = start + (c[threadIdx.x] ? atomicAdd(&fill[threadIdx.x], c[threadIdx.x]) : 0);
@@ -248,6 +250,14 @@ __global__ void k_fill(int64_t N, const int *__restrict__ atom_cell, const int *
     cell_atoms[slot] = (int)i;
 }
 
+// Sort key of a cell member: type in the top 4 bits (atom indices < 2^28); a
+// type outside [0, ntypes) gets 15, sorts last and is counted for no type.
+__device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
+{
+    const unsigned tt = (t >= 0 && t < ntypes) ? (unsigned)t : 15u;
+    return (unsigned)atom | (tt << 28);
+}
+
 // one thread per cell (all structures): insertion sort of the cell's member
 // list by (type, atom index), so the neighbour order does not depend on the
 // order of the atomic insertions, and the count of each type among the
@@ -265,45 +275,51 @@ __global__ void k_sort_cells(int S, const StructGrid *__restrict__ grid, const i
     if (n <= 64) {
         int key[64];
         for (int p = 0; p < n; ++p) {
-            const int v = a[p] | (type[a[p]] << 28);            // atom indices < 2^28, types < 8
+            const unsigned v = sort_key(a[p], type[a[p]], ntypes);
             int q = p - 1;
-            while (q >= 0 && key[q] > v) { key[q + 1] = key[q]; --q; }
-            key[q + 1] = v;
+            while (q >= 0 && (unsigned)key[q] > v) { key[q + 1] = key[q]; --q; }
+            key[q + 1] = (int)v;
         }
         int p = 0;
         for (int t = 0; t < ntypes; ++t) {
             int q = p;
-            while (q < n && (key[q] >> 28) == t) { a[q] = key[q] & 0x0fffffff; ++q; }
+            while (q < n && ((unsigned)key[q] >> 28) == (unsigned)t) { a[q] = key[q] & 0x0fffffff; ++q; }
             tc[t] = q - p;
             p = q;
         }
+        for (; p < n; ++p) a[p] = key[p] & 0x0fffffff;          // out-of-range types, last
         return;
     }
-    for (int p = 0; p < n; ++p) a[p] |= type[a[p]] << 28;
+    unsigned *u = reinterpret_cast<unsigned *>(a);
+    for (int p = 0; p < n; ++p) u[p] = sort_key(a[p], type[a[p]], ntypes);
     for (int p = 1; p < n; ++p) {
-        const int v = a[p];
+        const unsigned v = u[p];
         int q = p - 1;
-        while (q >= 0 && a[q] > v) { a[q + 1] = a[q]; --q; }
-        a[q + 1] = v;
+        while (q >= 0 && u[q] > v) { u[q + 1] = u[q]; --q; }
+        u[q + 1] = v;
     }
     int p = 0;
     for (int t = 0; t < ntypes; ++t) {
         int q = p;
-        while (q < n && (a[q] >> 28) == t) a[q++] &= 0x0fffffff;
+        while (q < n && (u[q] >> 28) == (unsigned)t) ++q;
         tc[t] = q - p;
         p = q;
     }
+    for (int q = 0; q < n; ++q) u[q] &= 0x0fffffffu;
 }
 
-// cell-ordered copy of the wrapped positions with the atom's type in .w, so the
+// cell-ordered copy of the wrapped positions with the atom's type in .w (-1
+// for a type outside [0, ntypes): such atoms are never neighbours), so the
 // neighbour search reads each cell's members contiguously
 __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const double *__restrict__ xw,
-                           const int *__restrict__ type, double4 *__restrict__ cell_pos)
+                           const int *__restrict__ type, int ntypes, double4 *__restrict__ cell_pos)
 {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= N) return;
     const int a = cell_atoms[s];
-    cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2], (double)type[a]);
+    const int t = type[a];
+    cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2],
+                               (t >= 0 && t < ntypes) ? (double)t : -1.0);
 }
 
 // Neighbour search, one thread block per cell.  Every atom of a cell has the
@@ -384,6 +400,12 @@ __device__ __forceinline__ void load_candidates(NeighShared &sh, int k0, int k1,
         const int slot = sh.start[lo] + k - sh.pre[lo];
         const double4 xj = cell_pos[slot];
         const int j = cell_atoms[slot];
+        if (xj.w < 0.0) {                                        // type out of range: never a neighbour
+            const double nan = __longlong_as_double(0x7ff8000000000000ll);
+            sh.c.x[s] = sh.c.y[s] = sh.c.z[s] = nan;
+            sh.c.jt[s] = 0;
+            continue;
+        }
         const int qp = sh.q[lo];
         const double Q0 = (qp & 255) - 128, Q1 = ((qp >> 8) & 255) - 128, Q2 = ((qp >> 16) & 255) - 128;
         sh.c.x[s] = xj.x + (R0 * Q0 + R3 * Q1 + R6 * Q2);
@@ -479,7 +501,7 @@ __device__ void search_atom_global(NeighShared &sh, int warp, int lane, int64_t 
                 const double dy = xi1 - (xj.y + (g.R[1] * Q0 + g.R[4] * Q1 + g.R[7] * Q2));
                 const double dz = xi2 - (xj.z + (g.R[2] * Q0 + g.R[5] * Q1 + g.R[8] * Q2));
                 const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12)) {
+                if (r2 < rc2 && ((int64_t)j != i || r2 > 1e-12) && xj.w >= 0.0) {
                     acc = true;
                     e = make_float4((float)dx, (float)dy, (float)dz, __int_as_float(j | ((int)xj.w << 28)));
                 }
@@ -728,7 +750,10 @@ __global__ void k_energy(const int64_t *__restrict__ off, const float *__restric
     double sum = 0.0;
     for (int64_t a = off[s] + threadIdx.x; a < off[s + 1]; a += blockDim.x) {
         sum += (double)e_atom[a];
-        if (vacuum) sum += vac[type[a]];
+        if (vacuum) {
+            const int t = type[a];
+            if (t >= 0 && t < pot->ntypes) sum += vac[t];
+        }
     }
     part[threadIdx.x] = sum;
     __syncthreads();
@@ -826,7 +851,7 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.cell_atoms.reserve(N));
     r(E.cell_pos.reserve(N));
     r(E.order.reserve(N));
-    r(E.type_fill.reserve(2 * NNP_MAX_TYPES));
+    r(E.type_fill.reserve(2 * (NNP_MAX_TYPES + 1)));
     r(E.nbr.reserve(N * (size_t)E.cap));
     r(E.nbr_cnt.reserve(N));
     r(E.G.reserve(N * (size_t)E.gstride));
@@ -848,10 +873,10 @@ std::string run_neighbors(Engine &E, int pbc)
     cudaStream_t st = E.stream;
     E.mark(0);
     E.launches += 12;
-    cudaMemsetAsync(E.type_fill.p, 0, 2 * NNP_MAX_TYPES * sizeof(int), st);
+    cudaMemsetAsync(E.type_fill.p, 0, 2 * (NNP_MAX_TYPES + 1) * sizeof(int), st);
     k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p);
     k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p,
-                                                               E.type_fill.p + NNP_MAX_TYPES, E.order.p);
+                                                               E.type_fill.p + NNP_MAX_TYPES + 1, E.order.p);
     k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
                                                              E.dpot.ntypes, E.err.p);
     k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
@@ -865,7 +890,8 @@ std::string run_neighbors(Engine &E, int pbc)
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
     k_sort_cells<<<grid_for((int64_t)cell_bound, 128, 1 << 30), 128, 0, st>>>(
         S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes, E.cell_atoms.p, E.cell_tcnt.p);
-    k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.cell_pos.p);
+    k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
+                                                          E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     const int nsm = sizeof(NeighShared);
     cudaFuncSetAttribute(k_neigh, cudaFuncAttributeMaxDynamicSharedMemorySize, nsm);
@@ -965,18 +991,21 @@ std::string run_energy(Engine &E, bool vacuum)
 
 // per-atom energies in FP64: the network energy of each atom, plus its
 // element's vacuum energy when requested (NNH::energy, nnh.cpp:207-210)
-__global__ void k_atom_energy(int64_t N, const float *__restrict__ e_atom, const int *__restrict__ type, int vacuum,
-                              const double *__restrict__ vac, double *__restrict__ out)
+__global__ void k_atom_energy(int64_t N, const float *__restrict__ e_atom, const int *__restrict__ type, int ntypes,
+                              int vacuum, const double *__restrict__ vac, double *__restrict__ out)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < N) out[i] = (double)e_atom[i] + (vacuum ? vac[type[i]] : 0.0);
+    if (i >= N) return;
+    const int t = type[i];
+    out[i] = (double)e_atom[i] + ((vacuum && t >= 0 && t < ntypes) ? vac[t] : 0.0);
 }
 
 std::string run_atom_energy(Engine &E, bool vacuum, double *out)
 {
     const int64_t N = E.n_atoms;
     if (N == 0) return "";
-    k_atom_energy<<<grid_for(N, 256, 1 << 30), 256, 0, E.stream>>>(N, E.e_atom.p, E.type.p, vacuum ? 1 : 0, E.vac.p, out);
+    k_atom_energy<<<grid_for(N, 256, 1 << 30), 256, 0, E.stream>>>(N, E.e_atom.p, E.type.p, E.dpot.ntypes,
+                                                                   vacuum ? 1 : 0, E.vac.p, out);
     E.launches += 1;
     return cuda_msg("per-atom energies");
 }

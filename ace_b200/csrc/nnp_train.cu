@@ -65,6 +65,7 @@ k_nn_train(i64 N, const DevPot *__restrict__ pot, const float *__restrict__ wpar
     const bool tan = (C != nullptr);
     for (i64 idx = blockIdx.x * (i64)WARPS + warp; idx < N; idx += (i64)gridDim.x * WARPS) {
         const i64 i = order[idx];
+        if ((unsigned)type[i] >= (unsigned)P.ntypes) continue;  // type out of range (reported by the call)
         const DevType &T = P.t[type[i]];
         const NetView Vw = net_view(w_s + T.woff, T);
         float *gt = g_s + T.woff;     // gradient accumulators, same layout as the weights
