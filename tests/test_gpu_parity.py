@@ -103,6 +103,23 @@ def test_free_boundaries(tmp_path):
         assert np.abs(F[b.atom_off[s]:b.atom_off[s + 1]] - fo).max() < F_ATOL
 
 
+def test_large_free_cluster(tmp_path):
+    """A 1500-atom cluster without periodic boundaries is one neighbour cell:
+    its candidate list (every atom) streams through the shared buffer in
+    chunks, and its atoms are processed in more than one round of kept
+    counts."""
+    b = synth.batch_random(61, [1500], 3)
+    b = synth.Batch(b.atom_off, b.pos, b.type, b.cell, pbc=False)
+    path = make_pot(tmp_path, 2, small_batch(2))
+    op = orc.OraclePot.from_file(path)
+    nn = NNP.read(path)
+    E, F = nn.compute_batch(b.atom_off, b.pos, b.type, None, pbc=False)
+    p, t, c = b.structure(0)
+    eo, fo, _ = orc.compute(op, p, t, np.zeros((3, 3)), pbc=False)
+    assert abs(E[0] - eo) / len(p) < E_ATOL
+    assert np.abs(F - fo).max() < F_ATOL
+
+
 def test_empty_and_ragged(tmp_path):
     """Empty structures inside a batch and single-atom structures."""
     b = small_batch(2, n=4)
