@@ -846,7 +846,7 @@ int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, co
     if (n_atoms > NNP_NOALLOC_MAX_ATOMS)
         return fail(h, NNP_ERR_CAPACITY, "allocation-free call takes at most " + std::to_string(NNP_NOALLOC_MAX_ATOMS) +
                                              " atoms, got " + std::to_string(n_atoms));
-    if (E.precision != NNP_PREC_FP32) return fail(h, NNP_ERR_UNSUPPORTED, "this build implements the FP32 network path only");
+    if (E.precision != NNP_PREC_FP32) return fail(h, NNP_ERR_UNSUPPORTED, "the allocation-free call runs the FP32 networks only (set precision to FP32)");
     int nin = 0;
     for (int t = 0; t < E.dpot.ntypes; ++t) nin = std::max(nin, E.dpot.t[t].n_input);
     if (gstride < nin) return fail(h, NNP_ERR_ARG, "gstride " + std::to_string(gstride) + " is below the largest input size " + std::to_string(nin));

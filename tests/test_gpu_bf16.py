@@ -2,8 +2,9 @@
 reference's own outputs (tests/golden/*.npz).
 
 Tolerances: BF16X3 (hi*hi + hi*lo + lo*hi, ~16 significant bits, FP32
-accumulation) -- 2e-5 eV/atom and 2e-4 eV/A, well inside the north-star
-bound of 1 meV/atom and 10 meV/A (measured <= 7e-6 eV/atom, 3.6e-5 eV/A).
+accumulation) -- 2e-5 eV/atom and 2e-4 eV/A, well inside the bound of
+1 meV/atom and 10 meV/A that the tensor-core networks are held to (measured
+<= 7e-6 eV/atom, 3.6e-5 eV/A).
 BF16 (one BF16 product per MMA) does NOT meet that bound on these inputs
 (measured up to 5.4 meV/atom and 20 meV/A: the conditioned network inputs
 and the weights each lose ~3 significant digits), so it is tested against
