@@ -766,7 +766,12 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
         if (ce != cudaSuccess) { rc = fail(h, NNP_ERR_CUDA, std::string("kernel failure: ") + cudaGetErrorString(ce)); break; }
         const nnp::DevErr er = *E.h_err;
         if (er.bad_type) { rc = fail(h, NNP_ERR_TYPE, "atom type index out of range"); break; }
-        if (er.bad_cell) { rc = fail(h, NNP_ERR_ARG, "a periodic cell has zero volume"); break; }
+        if (er.bad_cell == 1) { rc = fail(h, NNP_ERR_ARG, "a periodic cell has zero volume"); break; }
+        if (er.bad_cell) {
+            rc = fail(h, NNP_ERR_CAPACITY, "a periodic cell is thinner than rc/" + std::to_string(NNP_MAX_IMAGES) +
+                                               " in some direction (too many images to search)");
+            break;
+        }
         if (er.need_cap > E.cap) {
             if (er.need_cap > NNP_MAX_NBR) {
                 rc = fail(h, NNP_ERR_CAPACITY, "an atom has " + std::to_string(er.need_cap) + " neighbours; the device path handles up to " + std::to_string(NNP_MAX_NBR));

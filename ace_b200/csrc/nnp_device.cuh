@@ -20,6 +20,7 @@
 #define NNP_MAX_CUT 4         // distinct (cutoff form, rc) pairs in a potential
 #define NNP_MAX_NODES 128     // widest network layer handled on the device
 #define NNP_MAX_NBR 256       // neighbours per atom staged in shared memory
+#define NNP_MAX_IMAGES 64     // cell images searched on each side in one lattice direction
 
 #define NNP_WARPS 8           // warps per block of the per-atom kernels
 #define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
@@ -100,7 +101,7 @@ struct DevPot {
 struct DevErr {
     int need_cap;     // largest neighbour count seen (when above the capacity)
     int bad_type;     // an atom type was outside [0, ntypes)
-    int bad_cell;     // a periodic cell had no volume
+    int bad_cell;     // a periodic cell had no volume (1) or was thinner than rc / NNP_MAX_IMAGES (2)
     int nonfinite;    // a non-finite energy or force
 };
 

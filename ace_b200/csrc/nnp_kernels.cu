@@ -148,7 +148,12 @@ __global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *_
                 if (g.nc[2] > g.nc[k]) k = 2;
                 g.nc[k] = (g.nc[k] + 1) / 2;
             }
-            for (int n = 0; n < 3; ++n) g.m[n] = (int)ceil(rc * g.nc[n] / w[n]);
+            for (int n = 0; n < 3; ++n) g.m[n] = (int)fmin(ceil(rc * g.nc[n] / w[n]), 1e6);
+            if (g.m[0] > NNP_MAX_IMAGES || g.m[1] > NNP_MAX_IMAGES || g.m[2] > NNP_MAX_IMAGES) {
+                // thinner than rc / NNP_MAX_IMAGES in some direction: reported, not searched
+                atomicMax(&err->bad_cell, 2);
+                g.m[0] = g.m[1] = g.m[2] = 0;
+            }
         }
     }
     grid[s] = g;

@@ -157,6 +157,23 @@ def test_errors(tmp_path):
     assert ei.value.code == -1
 
 
+def test_thin_cell_reported(tmp_path):
+    """A periodic cell 0.05 A thick in one direction would need hundreds of
+    images on each side of every atom: the call reports it (capacity error)
+    instead of searching them."""
+    path = make_pot(tmp_path, 2)
+    nn = NNP.read(path)
+    pos = np.array([[1.0, 1.0, 0.01], [5.0, 5.0, 0.02]])
+    cell = np.array([[[10.0, 0.0, 0.0], [0.0, 10.0, 0.0], [0.0, 0.0, 0.05]]])
+    with pytest.raises(NNPError) as ei:
+        nn.compute_batch(np.array([0, 2]), pos, np.array([0, 1], dtype=np.int32), cell)
+    assert ei.value.code == -5 and "thinner" in str(ei.value)
+    # the handle stays usable
+    b = small_batch(2, n=2)
+    E, F = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    assert np.isfinite(E).all() and np.isfinite(F).all()
+
+
 def test_write_roundtrip(tmp_path):
     path = make_pot(tmp_path, 5)
     nn = NNP.read(path)
