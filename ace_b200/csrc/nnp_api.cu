@@ -957,6 +957,17 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
     return NNP_OK;
 }
 
+int nnp_set_loss(nnp_handle *h, int32_t kind, double delta)
+{
+    if (!h) return NNP_ERR_ARG;
+    if (kind < NNP_LOSS_MSE || kind > NNP_LOSS_ASINH) return fail(h, NNP_ERR_ARG, "Invalid loss.");
+    if ((kind == NNP_LOSS_HUBER || kind == NNP_LOSS_ASINH) && !(delta > 0.0 && std::isfinite(delta)))
+        return fail(h, NNP_ERR_ARG, "the loss width delta must be positive and finite");
+    h->E.loss_kind = kind;
+    h->E.loss_delta = delta;
+    return NNP_OK;
+}
+
 int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, const double *f_ref, double w_f,
                    int32_t norm_mode, double *loss, double *grad, double *e_out, double *f_out, uint32_t flags)
 {
@@ -998,9 +1009,29 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, c
         case 4: nrm = 1.0 / (std::log(nat) + 1.0); break;
         default: break;
         }
+        // energy term: NNPTEFR::error_cost_o1's loss and gradient factor (nnptefr.cpp:1340-1376)
         const double dU = (Eh[s] - e_ref[s]) * nrm;
-        L += bi * 0.5 * dU * dU;
-        const double gf = nrm * dU * bi;
+        double gf = nrm * bi;
+        switch (E.loss_kind) {
+        case NNP_LOSS_MAE:
+            L += bi * std::fabs(dU);
+            gf *= (dU > 0) - (dU < 0);
+            break;
+        case NNP_LOSS_HUBER: {
+            const double arg = dU / E.loss_delta, sq = std::sqrt(1.0 + arg * arg);
+            L += bi * E.loss_delta * E.loss_delta * (sq - 1.0);
+            gf *= dU / sq;
+        } break;
+        case NNP_LOSS_ASINH: {
+            const double arg = dU / E.loss_delta, sq = std::sqrt(1.0 + arg * arg), lg = std::log(arg + sq);
+            L += bi * E.loss_delta * E.loss_delta * (1.0 - sq + arg * lg);
+            gf *= lg * E.loss_delta;
+        } break;
+        default:
+            L += bi * 0.5 * dU * dU;
+            gf *= dU;
+            break;
+        }
         const double fs = nat > 0 ? w_f / (3.0 * nat) : 0.0;
         double lf = 0.0;
         for (int64_t a = a0; a < a1; ++a) {

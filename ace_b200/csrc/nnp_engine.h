@@ -101,6 +101,8 @@ struct Engine {
     DBuf<float> gE;               // per-atom energy factor
     DBuf<float> tang;             // tangent symmetry functions C [N * gstride]
     DBuf<double> pgrad;           // parameter gradient in the wpar layout [wfloats]
+    int loss_kind = 1;            // energy-loss kind of nnp_train_grad (NNP_LOSS_*)
+    double loss_delta = 1.0;      // its width (HUBER, ASINH)
     DevErr *h_err = nullptr;      // pinned
     // pinned staging for host-pointer calls
     void *h_stage = nullptr;

@@ -22,6 +22,7 @@ NNP_OK = 0
 ERRORS = {-1: "ARG", -2: "IO", -3: "PARSE", -4: "CUDA", -5: "CAPACITY", -6: "UNSUPPORTED", -7: "TYPE",
           -8: "NOT_FINITE"}
 PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
+LOSS_MSE, LOSS_MAE, LOSS_HUBER, LOSS_ASINH = 1, 2, 3, 4   # opt::Loss (opt/loss.hpp:18-24)
 ENERGY, FORCES, VACUUM, DEVICE_PTRS, SYMM = 1, 2, 4, 8, 16
 
 
@@ -66,6 +67,7 @@ def lib():
             "nnp_get_params": ([p, p], i),
             "nnp_set_params": ([p, p], i),
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
+            "nnp_set_loss": ([p, i, d], i),
             "nnp_set_accumulation": ([p, i], i),
             "nnp_set_specialization": ([p, i], i),
             "nnp_specialization": ([p, C.POINTER(i), C.POINTER(C.c_char_p)], i),
@@ -167,6 +169,11 @@ class NNP:
 
     def set_precision(self, prec: int):
         self._check(lib().nnp_set_precision(self._h, prec))
+
+    def set_loss(self, kind: int, delta: float = 1.0):
+        """Energy-loss kind of train_grad (LOSS_MSE, LOSS_MAE, LOSS_HUBER,
+        LOSS_ASINH) and its width, as nnptefr's loss / delta settings."""
+        self._check(lib().nnp_set_loss(self._h, kind, float(delta)))
 
     def set_graphs(self, on: bool = True):
         """Replay the device-side step as a CUDA graph while calls repeat their shape."""

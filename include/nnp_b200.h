@@ -176,9 +176,11 @@ int nnp_get_params(const nnp_handle *h, double *params);
 int nnp_set_params(nnp_handle *h, const double *params);
 
 /* Energy(+force) loss and its gradient with respect to all network parameters.
- * The energy term is NNPTEFR::error_cost_o1's MSE term (nnptefr.cpp:1292-1347,
- * batch average nnptefr.cpp:996-1000); the force term has no reference
- * counterpart (nnptefr trains on energies only):
+ * The energy term is NNPTEFR::error_cost_o1's (nnptefr.cpp:1292-1380, batch
+ * average nnptefr.cpp:996-1000), MSE unless nnp_set_loss picks another kind;
+ * the force term has no reference counterpart in nnptefr (which trains on
+ * energies only; its second derivatives are the reference's NN::D2ODZDI,
+ * ml/nn.cpp:2047-2137, contracted with dG/dr):
  *   L = (1/B) sum_s [ 0.5*(norm_s*(E_s - e_ref_s))^2
  *                     + w_f * 0.5/(3 N_s) * sum_i |F_i - f_ref_i|^2 ]
  * E_s excludes vacuum energies (nnptefr subtracts them from the labels,
@@ -188,6 +190,19 @@ int nnp_set_params(nnp_handle *h, const double *params);
 int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);
+
+/* Energy-loss kind of nnp_train_grad, opt::Loss (opt/loss.hpp:18-24) as
+ * NNPTEFR::error_cost_o1 applies it to dU = norm_s (E_s - e_ref_s)
+ * (nnptefr.cpp:1340-1376): MSE 0.5 dU^2 (the default), MAE |dU|,
+ * HUBER delta^2 (sqrt(1 + (dU/delta)^2) - 1),
+ * ASINH delta^2 (1 - sqrt(1 + a^2) + a asinh(a)), a = dU/delta.
+ * The force term stays the MSE of nnp_train_grad.  delta (> 0) is used by
+ * HUBER and ASINH only. */
+#define NNP_LOSS_MSE 1
+#define NNP_LOSS_MAE 2
+#define NNP_LOSS_HUBER 3
+#define NNP_LOSS_ASINH 4
+int nnp_set_loss(nnp_handle *h, int32_t kind, double delta);
 
 /* Allocation-free energies from device-resident symmetry functions (no
  * counterpart in the reference, whose NNP::compute_energy (nnp.cpp:329-338)

@@ -920,6 +920,33 @@ static double orc_norm(int mode, double n)
     }
 }
 
+/* Loss of one structure's scaled energy error dU and its derivative
+ * dloss/ddU (*dl), NNPTEFR::error_cost_o1 (nnptefr.cpp:1340-1376). */
+static double orc_loss(int kind, double delta, double dU, double *dl)
+{
+    switch (kind) {
+    case 2:
+        *dl = (dU > 0) - (dU < 0);
+        return fabs(dU);
+    case 3: {
+        const double arg = dU / delta, sq = sqrt(1.0 + arg * arg);
+        *dl = dU / sq;
+        return delta * delta * (sq - 1.0);
+    }
+    case 4: {
+        const double arg = dU / delta, sq = sqrt(1.0 + arg * arg), lg = log(arg + sq);
+        *dl = lg * delta;
+        return delta * delta * (1.0 - sq + arg * lg);
+    }
+    case 1:
+        *dl = dU;
+        return 0.5 * dU * dU;
+    default:
+        *dl = NAN;
+        return NAN;
+    }
+}
+
 static int orc_param_offsets(const orc_pot *p, int *off)
 {
     int tot = 0;
@@ -927,11 +954,12 @@ static int orc_param_offsets(const orc_pot *p, int *off)
     return tot;
 }
 
-/* NNPTEFR::error_cost_o1, MSE branch (nnptefr.cpp:1292-1347), then the batch
- * average of nnptefr.cpp:996-1000. */
+/* NNPTEFR::error_cost_o1 (nnptefr.cpp:1292-1380), then the batch average of
+ * nnptefr.cpp:996-1000. */
 double orc_energy_loss_grad(const orc_pot *p, int nstruct, const int64_t *atom_off,
                             const int32_t *type, int gstride, const double *symm,
-                            const double *e_ref, int norm_mode, double *grad)
+                            const double *e_ref, int norm_mode, int loss_kind, double delta,
+                            double *grad)
 {
     int off[64];
     const int np = orc_param_offsets(p, off);
@@ -956,9 +984,9 @@ double orc_energy_loss_grad(const orc_pot *p, int nstruct, const int64_t *atom_o
         const double nrm = orc_norm(norm_mode, nat);
         const double dE = pe - e_ref[s];
         const double dU = dE * nrm;
-        double gfac = nrm;
-        err += 0.5 * dU * dU;
-        gfac *= dU;
+        double dl;
+        err += orc_loss(loss_kind, delta, dU, &dl);
+        const double gfac = nrm * dl;
         for (int k = 0; k < np; ++k) grad[k] += gs[k] * gfac;
     }
     const double bi = 1.0 / nstruct;
@@ -1021,7 +1049,7 @@ static void orc_net_jvp_grad(const orc_net *nn, const orc_work *w, const double 
 double orc_ef_loss_grad(const orc_pot *p, int nstruct, const int64_t *atom_off,
                         const double *pos, const int32_t *type, const double *cell, int pbc,
                         const double *e_ref, const double *f_ref, double w_f, int norm_mode,
-                        double *grad, double *eout, double *fout)
+                        int loss_kind, double delta, double *grad, double *eout, double *fout)
 {
     static const double zero9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int T = p->ntypes, TT = T * (T + 1) / 2;
@@ -1060,7 +1088,8 @@ double orc_ef_loss_grad(const orc_pot *p, int nstruct, const int64_t *atom_off,
             lf += df * df;
             V[k] = fs * df * bi;
         }
-        loss += bi * (0.5 * dU * dU + 0.5 * fs * lf);
+        double dl;
+        loss += bi * (orc_loss(loss_kind, delta, dU, &dl) + 0.5 * fs * lf);
         if (grad) {
             /* c_a = sum_i dG_a/dx_i . v_i over every pair and triplet */
             for (int i = 0; i < nat; ++i) {
@@ -1103,7 +1132,7 @@ double orc_ef_loss_grad(const orc_pot *p, int nstruct, const int64_t *atom_off,
                 }
             }
             /* gradient: energy term g_s dE/dtheta, force term -d(dE/dG . c)/dtheta */
-            const double gfac = nrm * dU * bi;
+            const double gfac = nrm * dl * bi;
             for (int i = 0; i < nat; ++i) {
                 const int t = ts[i];
                 orc_net nn;

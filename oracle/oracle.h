@@ -108,25 +108,29 @@ double orc_ann_fpbp(const orc_pot *pot, int II, const double *inp, double *dodi)
 double orc_cost_grad(const orc_pot *pot, int II, const double *inp, double *grad);
 int orc_nparams(const orc_pot *pot, int II);
 
-/* ---- energy loss + gradient over a batch (nnptefr.cpp:1292-1347, MSE, the
+/* ---- energy loss + gradient over a batch (nnptefr.cpp:1292-1380, the
  * batch average of nnptefr.cpp:996-1000).  Structures are CSR by atom_off.
  * norm_mode: 0 IDENTITY, 1 LINEAR (1/N), 2 SQRT, 3 CBRT, 4 LOG (nnptefr.cpp:614-620).
+ * loss_kind: opt::Loss (opt/loss.hpp:18-24) 1 MSE, 2 MAE, 3 HUBER, 4 ASINH,
+ * width delta (HUBER, ASINH).
  * grad: sum over types of nparams(type), types in index order.  Returns loss. */
 double orc_energy_loss_grad(const orc_pot *pot, int nstruct, const int64_t *atom_off,
                             const int32_t *type, int gstride, const double *symm,
-                            const double *e_ref, int norm_mode, double *grad);
+                            const double *e_ref, int norm_mode, int loss_kind, double delta,
+                            double *grad);
 
 /* ---- energy + force loss and its weight gradient (the nnptefr energy term
- * plus a force-weighted MSE term):
+ * plus a force-weighted MSE term), for MSE:
  *   L = (1/B) sum_s [ 0.5*(norm_s*(E_s-E_ref_s))^2
  *                     + w_f * 0.5/(3 N_s) * sum_i |F_i - F_ref_i|^2 ]
+ * and the energy term of orc_energy_loss_grad's loss_kind otherwise.
  * E_s excludes vacuum energies (compute_force semantics, as nnptefr subtracts
  * them from the labels).  Positions/cells/types are per structure (CSR).
  * grad may be NULL.  Returns L; eout (nstruct) and fout (N x 3) optional. */
 double orc_ef_loss_grad(const orc_pot *pot, int nstruct, const int64_t *atom_off,
                         const double *pos, const int32_t *type, const double *cell, int pbc,
                         const double *e_ref, const double *f_ref, double w_f, int norm_mode,
-                        double *grad, double *eout, double *fout);
+                        int loss_kind, double delta, double *grad, double *eout, double *fout);
 
 #ifdef __cplusplus
 }

@@ -71,9 +71,9 @@ def lib():
         _lib.orc_nparams.restype = i
         _lib.orc_nparams.argtypes = [p, i]
         _lib.orc_energy_loss_grad.restype = d
-        _lib.orc_energy_loss_grad.argtypes = [p, i, p, p, i, p, p, i, p]
+        _lib.orc_energy_loss_grad.argtypes = [p, i, p, p, i, p, p, i, i, d, p]
         _lib.orc_ef_loss_grad.restype = d
-        _lib.orc_ef_loss_grad.argtypes = [p, i, p, p, p, p, i, p, p, d, i, p, p, p]
+        _lib.orc_ef_loss_grad.argtypes = [p, i, p, p, p, p, i, p, p, d, i, i, d, p, p, p]
     return _lib
 
 
@@ -347,18 +347,18 @@ def cost_grad(pot: OraclePot, II, inp):
     return out, g
 
 
-def energy_loss_grad(pot: OraclePot, atom_off, typ, symm, e_ref, norm_mode=1):
+def energy_loss_grad(pot: OraclePot, atom_off, typ, symm, e_ref, norm_mode=1, loss_kind=1, delta=1.0):
     atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
     typ = np.ascontiguousarray(typ, dtype=np.int32)
     symm = np.ascontiguousarray(symm, dtype=np.float64)
     e_ref = np.ascontiguousarray(e_ref, dtype=np.float64)
     g = np.zeros(pot.nparams_total())
     loss = lib().orc_energy_loss_grad(pot.ref, len(atom_off) - 1, _ptr(atom_off), _ptr(typ), symm.shape[1],
-                                      _ptr(symm), _ptr(e_ref), norm_mode, _ptr(g))
+                                      _ptr(symm), _ptr(e_ref), norm_mode, loss_kind, float(delta), _ptr(g))
     return loss, g
 
 
-def ef_loss_grad(pot: OraclePot, batch, e_ref, f_ref, w_f, norm_mode=1, want_grad=True):
+def ef_loss_grad(pot: OraclePot, batch, e_ref, f_ref, w_f, norm_mode=1, want_grad=True, loss_kind=1, delta=1.0):
     off = np.ascontiguousarray(batch.atom_off, dtype=np.int64)
     pos = np.ascontiguousarray(batch.pos, dtype=np.float64)
     typ = np.ascontiguousarray(batch.type, dtype=np.int32)
@@ -369,6 +369,6 @@ def ef_loss_grad(pot: OraclePot, batch, e_ref, f_ref, w_f, norm_mode=1, want_gra
     eo = np.zeros(batch.n_struct)
     fo = np.zeros((batch.n_atoms, 3))
     loss = lib().orc_ef_loss_grad(pot.ref, batch.n_struct, _ptr(off), _ptr(pos), _ptr(typ), _ptr(cell),
-                                  int(batch.pbc), _ptr(e_ref), _ptr(f_ref), float(w_f), norm_mode,
-                                  _ptr(g) if want_grad else None, _ptr(eo), _ptr(fo))
+                                  int(batch.pbc), _ptr(e_ref), _ptr(f_ref), float(w_f), norm_mode, loss_kind,
+                                  float(delta), _ptr(g) if want_grad else None, _ptr(eo), _ptr(fo))
     return loss, g, eo, fo

@@ -36,6 +36,11 @@ def lib():
         L.ref_nnp_ninput.argtypes = [p, C.c_int]
         L.ref_nnp_compute.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, C.c_int, dp, dp, dp, dp,
                                       C.c_char_p, C.c_int]
+        L.ref_nnp_nparams.argtypes = [p, C.c_int]
+        L.ref_energy_loss_grad.argtypes = [p, C.c_int, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int), dp, C.c_int,
+                                           dp, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, C.c_char_p, C.c_int]
+        L.ref_force_term_grad.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, dp, C.c_double, dp,
+                                          dp, C.c_char_p, C.c_int]
         _lib = L
     return _lib
 
@@ -85,3 +90,50 @@ class RefNNP:
         if rc != 0:
             raise RuntimeError("reference compute failed: " + err.value.decode())
         return float(e[0]), f[:n], float(ev[0]), (g[:n] if want_symm else None)
+
+
+    def nparams(self, t: int) -> int:
+        """ANN::size of type t's network."""
+        return int(lib().ref_nnp_nparams(self.h, t))
+
+    def nparams_total(self) -> int:
+        return sum(self.nparams(t) for t in range(self.ntypes))
+
+    def energy_loss_grad(self, batch, e_ref, norm_mode=1, loss_kind=1, delta=1.0):
+        """Energy-loss gradient of a batch through the reference's fpbp +
+        Cost::grad per atom and NNPTEFR::error_cost_o1's loss factors:
+        returns (loss, grad in the per-element packing, rmse, energies)."""
+        off = np.ascontiguousarray(batch.atom_off, dtype=np.int64)
+        pos = np.ascontiguousarray(batch.pos, dtype=np.float64)
+        typ = np.ascontiguousarray(batch.type, dtype=np.int32)
+        cell = np.ascontiguousarray(np.asarray(batch.cell).reshape(-1, 9), dtype=np.float64)
+        e_ref = np.ascontiguousarray(e_ref, dtype=np.float64)
+        g = np.zeros(self.nparams_total())
+        loss, rmse = np.zeros(1), np.zeros(1)
+        en = np.zeros(batch.n_struct)
+        err = C.create_string_buffer(512)
+        rc = lib().ref_energy_loss_grad(self.h, batch.n_struct, off.ctypes.data_as(C.POINTER(C.c_int64)), _dp(pos),
+                                        typ.ctypes.data_as(C.POINTER(C.c_int)), _dp(cell), int(batch.pbc),
+                                        _dp(e_ref), norm_mode, loss_kind, float(delta), _dp(g), _dp(loss),
+                                        _dp(rmse), _dp(en), err, len(err))
+        if rc != 0:
+            raise RuntimeError("reference energy-loss gradient failed: " + err.value.decode())
+        return float(loss[0]), g, float(rmse[0]), en
+
+    def force_term_grad(self, pos, types, cell, v, fd_h, pbc=True, want_tangent=False):
+        """sum_i d/dtheta (dE_i/dG_i . C_i) for one structure, C_i the change of
+        G_i along the displacement field v, from the reference's D2ODZDI and
+        central differences of its compute_symm (potential with inpw = 1)."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        cell = np.ascontiguousarray(cell if cell is not None else np.zeros(9), dtype=np.float64).reshape(9)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        g = np.zeros(self.nparams_total())
+        ct = np.zeros((n, self.gstride)) if want_tangent else None
+        err = C.create_string_buffer(512)
+        rc = lib().ref_force_term_grad(self.h, n, _dp(pos), types.ctypes.data_as(C.POINTER(C.c_int)), _dp(cell),
+                                       1 if pbc else 0, _dp(v), float(fd_h), _dp(g), _dp(ct), err, len(err))
+        if rc != 0:
+            raise RuntimeError("reference force-term gradient failed: " + err.value.decode())
+        return (g, ct) if want_tangent else g

@@ -1,5 +1,8 @@
 """Writes the golden fixtures of tests/golden/ from the reference itself.
 
+train_config3.npz holds the reference's own training gradients (see
+make_train).
+
 Each fixture holds a potential file (text, as NNP::write writes it), a small
 CSR batch of structures, and the reference's outputs for every structure:
 NNP::compute_force energy (no vacuum terms) and forces, NNP::compute_energy
@@ -86,7 +89,109 @@ def make(name, k, b, pbc, seed=1234):
                         forces=np.concatenate(F), symm=np.concatenate(Gs), config=np.array(k))
 
 
+# (norm mode, loss kind, delta) of the energy-loss gradients in train_config3.npz:
+# every nnptefr norm with MSE, then MAE / HUBER / ASINH with the LINEAR norm
+TRAIN_CASES = [(0, 1, 1.0), (1, 1, 1.0), (2, 1, 1.0), (3, 1, 1.0), (4, 1, 1.0),
+               (1, 2, 1.0), (1, 3, 0.05), (1, 4, 0.05)]
+TRAIN_W_F = 0.5
+
+
+def fold_input_scaling(pot):
+    """The same networks with inpw = 1, inpb = 0: the input scale and bias
+    moved into the first layer (W0' = W0 diag(inpw), b0' = b0 + W0 (inpw * inpb))."""
+    for net in pot.nets:
+        w0 = net.w[0]
+        net.b[0] = net.b[0] + w0 @ (net.inpw * net.inpb)
+        net.w[0] = w0 * net.inpw[None, :]
+        net.inpw = np.ones_like(net.inpw)
+        net.inpb = np.zeros_like(net.inpb)
+    return pot
+
+
+def make_train():
+    """Training configuration 3 (two elements, 48-32-32-1 tanh) on 4 small
+    structures, labels from a teacher potential (other seed) evaluated by the
+    reference plus Gaussian noise (1 meV/atom, 20 meV/A).
+
+    potential_e: conditioned potential (inpw != 1).  For each case of
+    TRAIN_CASES, grad_e[c] / loss_e[c] are the reference's energy-loss gradient
+    and loss: NNP::compute_symm, then ANN::fpbp + Cost::grad per atom and
+    NNPTEFR::error_cost_o1's loss factor and batch average (ref_energy_loss_grad).
+
+    potential_f: the same networks with the input scaling folded into the
+    first layer (inpw = 1, for which the reference's D2ODZDI is exact).
+    grad_ef / loss_ef: the energy(MSE, LINEAR)+force loss with w_f = TRAIN_W_F,
+    the energy term as above and the force term -sum_i d/dtheta(dE_i/dG_i . C_i)
+    from the reference's D2ODZDI contracted with C_i, the change of the
+    reference's compute_symm along the force adjoint (central differences,
+    largest displacement 1e-5 A)."""
+    import tempfile
+    rng = np.random.default_rng(31)
+    b = synth.batch_random(31, rng.integers(16, 40, size=4), 2)
+    cb = conditioning_batch(3)
+    pots = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, seed in (("model", 5), ("teacher", 6)):
+            pot = synth.potential_config(3, seed=seed)
+            path = os.path.join(d, name + ".nnp")
+            potential.write(path, pot)
+            rp = ref.RefNNP(path)
+            G = np.concatenate([rp.compute(*cb.structure(s), want_symm=True)[3] for s in range(cb.n_struct)])
+            rp.close()
+            synth.condition(pot, G, cb.type)
+            potential.write(path, pot)
+            pots[name] = path
+        rt = ref.RefNNP(pots["teacher"])
+        Et, Ft = [], []
+        for s in range(b.n_struct):
+            e, f, _, _ = rt.compute(*b.structure(s))
+            Et.append(e)
+            Ft.append(f)
+        rt.close()
+        nat = np.diff(b.atom_off)
+        e_ref = np.array(Et) + rng.normal(0, 1e-3, size=b.n_struct) * nat
+        f_ref = np.concatenate(Ft) + rng.normal(0, 0.02, size=(b.n_atoms, 3))
+        text_e = open(pots["model"]).read()
+        rp = ref.RefNNP(pots["model"])
+        grad_e, loss_e = [], []
+        for nm, kind, delta in TRAIN_CASES:
+            L, g, _, _ = rp.energy_loss_grad(b, e_ref, norm_mode=nm, loss_kind=kind, delta=delta)
+            grad_e.append(g)
+            loss_e.append(L)
+        rp.close()
+        pot = fold_input_scaling(potential.read(pots["model"]))
+        path_f = os.path.join(d, "folded.nnp")
+        potential.write(path_f, pot)
+        text_f = open(path_f).read()
+        rp = ref.RefNNP(path_f)
+        L_e, g, _, _ = rp.energy_loss_grad(b, e_ref, norm_mode=1, loss_kind=1)
+        B = b.n_struct
+        lf = 0.0
+        for s in range(B):
+            p, t, c = b.structure(s)
+            a0, a1 = int(b.atom_off[s]), int(b.atom_off[s + 1])
+            _, f, _, _ = rp.compute(p, t, c)
+            df = f - f_ref[a0:a1]
+            fs = TRAIN_W_F / (3.0 * (a1 - a0))
+            lf += 0.5 * fs * float((df * df).sum()) / B
+            v = fs * df / B
+            g -= rp.force_term_grad(p, t, c, v, 1e-5 / np.abs(v).max())
+        rp.close()
+    np.savez_compressed(os.path.join(HERE, "train_config3.npz"),
+                        potential_e=np.frombuffer(text_e.encode(), dtype=np.uint8),
+                        potential_f=np.frombuffer(text_f.encode(), dtype=np.uint8),
+                        atom_off=b.atom_off, pos=b.pos, type=b.type, cell=np.asarray(b.cell).reshape(-1, 9),
+                        e_ref=e_ref, f_ref=f_ref, cases=np.array(TRAIN_CASES), grad_e=np.array(grad_e),
+                        loss_e=np.array(loss_e), w_f=np.array(TRAIN_W_F), grad_ef=g, loss_ef=np.array(L_e + lf))
+
+
 if __name__ == "__main__":
+    which = sys.argv[1:]
     for name, k, b, pbc in cases():
+        if which and name not in which:
+            continue
         make(name, k, b, pbc)
         print("wrote", name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
+    if not which or "train_config3" in which:
+        make_train()
+        print("wrote train_config3", os.path.getsize(os.path.join(HERE, "train_config3.npz")), "bytes")

@@ -1,7 +1,9 @@
 """Weight gradient of the energy(+force) loss on the GPU (nnp_train_grad)
-against the FP64 oracle (orc_ef_loss_grad, whose energy term follows
-NNPTEFR::error_cost_o1 and is checked against finite differences in
-test_oracle.py).
+against the reference's own analytic gradient (tests/golden/train_config3.npz:
+ANN::fpbp + Cost::grad with error_cost_o1's loss factors for the energy term,
+D2ODZDI contracted with dG/dr for the force term) and against the FP64
+oracle (orc_ef_loss_grad, which reproduces that fixture, tests/
+test_train_golden.py, and finite differences, test_oracle.py).
 
 Training configuration 3: two elements, 48-32-32-1 tanh networks; labels from
 a teacher potential of the same architecture (different seed) plus Gaussian
@@ -10,10 +12,13 @@ noise (1 meV/atom on energies, 20 meV/A on forces).
 Tolerances (FP32 device arithmetic, FP64 sums across blocks): loss 1e-5
 relative; gradient 1e-3 relative in the L2 norm and 1e-3 of the largest
 component elementwise."""
+import os
+
 import numpy as np
 import pytest
 
 from ace_b200 import NNP, NNPError, potential, synth
+from ace_b200.nnp import LOSS_MSE
 from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
@@ -88,4 +93,64 @@ def test_train_grad_errors(tmp_path):
         nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, 0.5, norm_mode=9)
     with pytest.raises(NNPError):
         nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, -1.0)
+    nn.close()
+
+
+def load_fixture(tmp_path):
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "train_config3.npz"))
+    paths = {}
+    for k in ("potential_e", "potential_f"):
+        p = str(tmp_path / (k + ".nnp"))
+        with open(p, "wb") as f:
+            f.write(z[k].tobytes())
+        paths[k] = p
+    b = synth.Batch(z["atom_off"], z["pos"], z["type"], z["cell"].reshape(-1, 3, 3), True)
+    return z, paths, b
+
+
+@pytest.mark.parametrize("jit", [True, False], ids=["specialised", "generic"])
+def test_energy_loss_grad_matches_reference_gradient(tmp_path, jit):
+    """Every norm mode and loss kind (MSE, MAE, HUBER, ASINH) against the
+    reference's Cost::grad / error_cost_o1 gradient of the fixture."""
+    z, paths, b = load_fixture(tmp_path)
+    nn = NNP.read(paths["potential_e"])
+    nn.set_specialization(jit)
+    f0 = np.zeros((b.n_atoms, 3))
+    for c, (nm, kind, delta) in enumerate(z["cases"]):
+        nn.set_loss(int(kind), float(delta))
+        L, g, _, _ = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, z["e_ref"], f0, 0.0, norm_mode=int(nm))
+        gr = z["grad_e"][c]
+        print("norm %d loss %d: loss %.6e vs %.6e, grad rel L2 %.2e" % (nm, kind, L, z["loss_e"][c], rel(g, gr)))
+        assert abs(L - z["loss_e"][c]) <= L_RTOL * abs(z["loss_e"][c])
+        assert rel(g, gr) < G_RTOL
+        assert np.abs(g - gr).max() < G_RTOL * np.abs(gr).max()
+    nn.set_loss(LOSS_MSE)
+    nn.close()
+
+
+@pytest.mark.parametrize("jit", [True, False], ids=["specialised", "generic"])
+def test_energy_force_loss_grad_matches_reference_gradient(tmp_path, jit):
+    """Energy + force loss (w_f = 0.5) against the reference's gradient: its
+    Cost::grad energy term plus its D2ODZDI force term."""
+    z, paths, b = load_fixture(tmp_path)
+    nn = NNP.read(paths["potential_f"])
+    nn.set_specialization(jit)
+    L, g, _, _ = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, z["e_ref"], z["f_ref"], float(z["w_f"]),
+                               norm_mode=1)
+    nn.close()
+    gr = z["grad_ef"]
+    print("loss %.6e vs %.6e, grad rel L2 %.2e, max %.2e" %
+          (L, float(z["loss_ef"]), rel(g, gr), np.abs(g - gr).max() / np.abs(gr).max()))
+    assert abs(L - float(z["loss_ef"])) <= L_RTOL * abs(float(z["loss_ef"]))
+    assert rel(g, gr) < G_RTOL
+    assert np.abs(g - gr).max() < G_RTOL * np.abs(gr).max()
+
+
+def test_set_loss_errors(tmp_path):
+    z, paths, b = load_fixture(tmp_path)
+    nn = NNP.read(paths["potential_e"])
+    with pytest.raises(NNPError):
+        nn.set_loss(0)
+    with pytest.raises(NNPError):
+        nn.set_loss(3, 0.0)
     nn.close()
