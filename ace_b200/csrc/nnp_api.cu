@@ -957,6 +957,15 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
     return NNP_OK;
 }
 
+int nnp_set_mma_wait(nnp_handle *h, int64_t polls)
+{
+    if (!h) return NNP_ERR_ARG;
+    if (polls < 0 || polls > 0xffffffffll) return fail(h, NNP_ERR_ARG, "polls must be in [0, 2^32)");
+    h->E.mma_wait_polls = (uint32_t)polls;
+    h->E.graph_release();       // a captured step holds the old bound
+    return NNP_OK;
+}
+
 int nnp_set_loss(nnp_handle *h, int32_t kind, double delta)
 {
     if (!h) return NNP_ERR_ARG;

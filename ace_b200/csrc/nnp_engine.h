@@ -58,6 +58,7 @@ struct Engine {
     int64_t wfloats = 0;
     int gstride = 0;              // row length of G / dE/dG (max n_input rounded up to 4)
     int precision = 0;
+    uint32_t mma_wait_polls = 0;  // bound of one tensor-core MMA-chain wait (0: the kernel's default)
     bool acc64 = false;           // FP64 running sums of the symmetry functions
     std::vector<float2> rpar_host;
     std::vector<float4> apar_host;

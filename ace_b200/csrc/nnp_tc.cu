@@ -28,7 +28,7 @@ namespace {
 
 constexpr int TILE = 128;
 constexpr uint32_t TMEM_COLS = 128;          // widest padded layer (NNP_MAX_NODES)
-constexpr uint32_t WAIT_POLLS = 1u << 26;     // bounded mbarrier wait (~0.1-1 s)
+constexpr uint32_t WAIT_POLLS = 1u << 26;     // default bound of one MMA-chain wait (~0.1-1 s); the final drain always uses it
 constexpr int HEADER = 128;                   // mbarrier (8 B) and TMEM address slot (4 B); operands follow
 
 __host__ __device__ inline int pad16(int n) { return (n + 15) & ~15; }
@@ -141,8 +141,13 @@ __device__ __forceinline__ void tc_activation(int neuron, float c, float z, floa
 }
 
 // One MMA chain D[128 x N] = A[128 x K] * B[N x K]^T issued by thread 0 and
-// waited for by every thread.  Returns false when the wait gave up.
-__device__ bool gemm(const Smem &s, int a_off, int b_off, int K, int N, bool split, uint32_t tmem, uint32_t &phase)
+// waited for by every thread, at most `polls` tests of the barrier each.
+// The result is the same in every thread of the block (a wait that gave up
+// in any thread fails it for all), so the block leaves its tile loop as one
+// and no thread is left at a barrier the others skip.  On failure the phase
+// is not advanced: the drain before the TMEM release waits for that chain.
+__device__ bool gemm(const Smem &s, int a_off, int b_off, int K, int N, bool split, uint32_t tmem, uint32_t &phase,
+                     uint32_t polls)
 {
     tc::fence_async_smem();
     tc::fence_before_sync();
@@ -166,8 +171,8 @@ __device__ bool gemm(const Smem &s, int a_off, int b_off, int K, int N, bool spl
         }
         tc::mma_commit(s.bar);
     }
-    const bool ok = tc::mbar_wait(s.bar, phase, WAIT_POLLS);
-    phase ^= 1u;
+    const bool ok = __syncthreads_and(tc::mbar_wait(s.bar, phase, polls)) != 0;
+    if (ok) phase ^= 1u;
     tc::fence_after_sync();
     return ok;
 }
@@ -178,7 +183,7 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, const float *__restrict__ wpar,
                                                 const int *__restrict__ type_count, const int *__restrict__ order,
                                                 const float *__restrict__ G, int gstride, float *__restrict__ e_atom,
-                                                float *__restrict__ dEdG, DevErr *err)
+                                                float *__restrict__ dEdG, DevErr *err, uint32_t polls)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const DevPot &P = *pot;
@@ -324,7 +329,7 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
         float e = 0.f;
         for (int h = 0; h + 1 < L && ok; ++h) {
             const int no = DT.nodes[h + 1], Po = p.P[h + 1];
-            ok = gemm(s, p.tile[h], p.wf[h], p.P[h], Po, SPLIT, tmem, phase);
+            ok = gemm(s, p.tile[h], p.wf[h], p.P[h], Po, SPLIT, tmem, phase, polls);
             if (!ok) break;
             const bool last = (h + 2 == L);
             int doff = 0, boff = 2 * nin;
@@ -377,7 +382,7 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
         // D_h sits in region h with K = P_{h+1}
         for (int h = L - 2; h >= 0 && ok; --h) {
             const int Pi = p.P[h], Po = p.P[h + 1];
-            ok = gemm(s, p.tile[h], p.wb[h], Po, Pi, SPLIT, tmem, phase);
+            ok = gemm(s, p.tile[h], p.wb[h], Po, Pi, SPLIT, tmem, phase, polls);
             if (!ok) break;
             if (h > 0) {
                 int doff = 0;
@@ -438,8 +443,9 @@ __global__ void __launch_bounds__(TILE) k_nn_tc(const DevPot *__restrict__ pot, 
         }
     }
     if (!ok && t == 0) atomicMax(&err->nonfinite, 2);
-    // every issued MMA chain was waited for unless a wait gave up; then wait
-    // once more, bounded, before the TMEM is released
+    // every issued MMA chain was waited for unless a wait gave up (in every
+    // thread alike); then the chain still in flight is waited for once more,
+    // with the full default bound, before the TMEM is released
     if (!ok) tc::mbar_wait(s0.bar, phase, WAIT_POLLS);
     tc::fence_before_sync();
     __syncthreads();
@@ -477,14 +483,15 @@ std::string run_nn_tc(Engine &E, bool split)
     const int per_sm = std::max(1, std::min(4, (228 * 1024) / (sm + 1024)));
     const int64_t tiles = (N + TILE - 1) / TILE + E.dpot.ntypes;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)nsm * per_sm));
+    const uint32_t polls = E.mma_wait_polls > 0 ? E.mma_wait_polls : WAIT_POLLS;
     if (split) {
         cudaFuncSetAttribute(k_nn_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         k_nn_tc<true><<<grid, TILE, sm, E.stream>>>(E.d_pot, E.wpar.p, E.type_fill.p, E.order.p, E.G.p, E.gstride,
-                                                   E.e_atom.p, E.dEdG.p, E.err.p);
+                                                   E.e_atom.p, E.dEdG.p, E.err.p, polls);
     } else {
         cudaFuncSetAttribute(k_nn_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         k_nn_tc<false><<<grid, TILE, sm, E.stream>>>(E.d_pot, E.wpar.p, E.type_fill.p, E.order.p, E.G.p, E.gstride,
-                                                    E.e_atom.p, E.dEdG.p, E.err.p);
+                                                    E.e_atom.p, E.dEdG.p, E.err.p, polls);
     }
     E.launches += 1;
     E.mark(3);

@@ -68,6 +68,7 @@ def lib():
             "nnp_set_params": ([p, p], i),
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
             "nnp_set_loss": ([p, i, d], i),
+            "nnp_set_mma_wait": ([p, C.c_int64], i),
             "nnp_set_accumulation": ([p, i], i),
             "nnp_set_specialization": ([p, i], i),
             "nnp_specialization": ([p, C.POINTER(i), C.POINTER(C.c_char_p)], i),
@@ -174,6 +175,10 @@ class NNP:
         """Energy-loss kind of train_grad (LOSS_MSE, LOSS_MAE, LOSS_HUBER,
         LOSS_ASINH) and its width, as nnptefr's loss / delta settings."""
         self._check(lib().nnp_set_loss(self._h, kind, float(delta)))
+
+    def set_mma_wait(self, polls: int):
+        """Bound of each tensor-core MMA-chain wait (0: the default)."""
+        self._check(lib().nnp_set_mma_wait(self._h, int(polls)))
 
     def set_graphs(self, on: bool = True):
         """Replay the device-side step as a CUDA graph while calls repeat their shape."""

@@ -92,6 +92,14 @@ int nnp_write(const nnp_handle *h, const char *path);
 /* Network-layer precision (NNP_PREC_*). */
 int nnp_set_precision(nnp_handle *h, int32_t precision);
 
+/* Bound of each wait of the tensor-core network kernel for one MMA chain, in
+ * tests of its barrier (no reference counterpart; 0 = the default, ~2^26
+ * tests, well above any chain's time).  A wait that runs out makes the call
+ * return NNP_ERR_CUDA ("an MMA wait timed out") instead of hanging; the
+ * kernel then waits for the chain in flight (default bound) and releases its
+ * tensor memory, so the handle stays usable. */
+int nnp_set_mma_wait(nnp_handle *h, int64_t polls);
+
 /* Running sums of the symmetry functions: NNP_ACC_FP64 adds every
  * FP32 pair/triplet term into an FP64 sum; NNP_ACC_FP32 (default) keeps FP32 sums
  * (faster; ~sqrt(T/32) ulp error for T triplets per atom). */

@@ -96,3 +96,31 @@ def test_bf16x3_many_tiles_four_elements(tmp_path):
         assert (np.abs(E1 - E0) / nat).max() < 5e-5
         assert np.abs(F1 - F0).max() < 5e-4
     nn.close()
+
+
+def test_mma_wait_timeout_returns_error_and_handle_recovers(tmp_path):
+    """A tensor-core wait that runs out ends the call with NNP_ERR_CUDA, not a
+    hang: with a bound of one barrier test per MMA chain every wait gives up
+    (a chain takes far longer than one test), the block leaves its tile loop
+    as one, drains the chain in flight and frees its tensor memory.  The same
+    handle then gives the reference's results with the default bound."""
+    from ace_b200 import NNPError
+    from ace_b200.nnp import ERRORS
+    path = [p for p in GOLDEN if p.endswith("config2.npz")][0]
+    z = np.load(path)
+    pot_path = str(tmp_path / "pot.nnp")
+    with open(pot_path, "wb") as f:
+        f.write(z["potential"].tobytes())
+    nn = NNP.read(pot_path)
+    nn.set_precision(2)
+    nn.set_mma_wait(1)
+    for _ in range(2):
+        with pytest.raises(NNPError) as ei:
+            nn.compute_batch(z["atom_off"], z["pos"], z["type"], z["cell"])
+        assert ERRORS[ei.value.code] == "CUDA" and "timed out" in str(ei.value)
+    nn.set_mma_wait(0)
+    E, F = nn.compute_batch(z["atom_off"], z["pos"], z["type"], z["cell"])
+    nn.close()
+    nat = np.maximum(np.diff(z["atom_off"]), 1)
+    assert (np.abs(E - z["energy"]) / nat).max() < PREC["bf16x3"][1]
+    assert np.abs(F - z["forces"]).max() < PREC["bf16x3"][2]
