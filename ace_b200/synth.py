@@ -92,29 +92,59 @@ def xavier_net(rng: np.random.Generator, nodes: Sequence[int], neuron: str = "TA
 
 
 def make_potential(ntypes: int, rc: float, n_rad: int, ang_sizes: Sequence[int], hidden: Sequence[int],
-                   seed: int, neuron: str = "TANH", cut: str = "COS",
-                   energies: Optional[Sequence[float]] = None) -> Potential:
+                   seed: int, neuron="TANH", cut: str = "COS",
+                   energies: Optional[Sequence[float]] = None, rform: str = "GAUSSIAN",
+                   aform: str = "GAUSS") -> Potential:
     """ntypes elements, n_rad radial functions per neighbour element, angular
-    block sizes in TensorTri order (len = ntypes*(ntypes+1)/2)."""
+    block sizes in TensorTri order (len = ntypes*(ntypes+1)/2).  neuron is one
+    activation name for every element's network or a list of one per element;
+    rform / aform name the radial / angular form (basis_radial.hpp:27-35,
+    basis_angular.hpp:27-35), cut the cutoff (cutoff.hpp:23-29)."""
     TT = ntypes * (ntypes + 1) // 2
     if len(ang_sizes) != TT:
         raise ValueError("need %d angular block sizes" % TT)
+    neurons = [neuron] * ntypes if isinstance(neuron, str) else list(neuron)
+    if len(neurons) != ntypes:
+        raise ValueError("need one activation per element")
     rng = np.random.default_rng(seed)
     types = [ElementType(name=NAMES[i], energy=(energies[i] if energies else -1.0 - 0.5 * i),
                          mass=1.0 + i) for i in range(ntypes)]
     rs = np.linspace(0.5, min(6.0, rc), n_rad) if n_rad > 1 else np.array([0.5])
-    basis_r = [[BasisR(cut, rc, "GAUSSIAN", rs.copy(), np.ones(n_rad)) for _ in range(ntypes)]
+    basis_r = [[BasisR(cut, rc, rform, rs.copy(), np.ones(n_rad)) for _ in range(ntypes)]
                for _ in range(ntypes)]
     basis_a = []
     for _ in range(ntypes):
         row = []
         for t in range(TT):
             e, z, l = angular_params(ang_sizes[t])
-            row.append(BasisA(cut, rc, "GAUSS", e, z, l))
+            row.append(BasisA(cut, rc, aform, e, z, l))
         basis_a.append(row)
     nin = ntypes * n_rad + sum(ang_sizes)
-    nets = [xavier_net(rng, [nin] + list(hidden) + [1], neuron) for _ in range(ntypes)]
+    nets = [xavier_net(rng, [nin] + list(hidden) + [1], neurons[i]) for i in range(ntypes)]
     return Potential(types, rc, basis_r, basis_a, nets)
+
+
+# Potentials of the other basis forms, cutoffs and activations the reference
+# supports, two or three elements each (6 radial functions per neighbour
+# element, 4 angular per block, 24-16-16-1 or 30-16-16-1 networks):
+# name -> (cutoff, radial form, angular form, activation of each element)
+FORM_POTENTIALS = {
+    "forms_sech_gauss2": ("TANH", "SECH", "GAUSS2", ["SIGMOID", "SWISH"]),
+    "forms_logistic_sech": ("POLY3", "LOGISTIC", "SECH", ["GELU", "SOFTPLUS"]),
+    "forms_tanh_student3": ("COS", "TANH", "STUDENT3", ["ISRU", "ARCTAN"]),
+    "forms_logcosh_student4": ("TANH", "LOGCOSH", "STUDENT4", ["ELU", "MISH"]),
+    "forms_logcosh2_student5": ("POLY3", "LOGCOSH2", "STUDENT5", ["PFLU", "LOGISH"]),
+    "forms_step_gauss": ("STEP", "GAUSSIAN", "GAUSS", ["SQPLUS", "ATISH"]),
+    "forms_activations": ("COS", "GAUSSIAN", "GAUSS", ["IERF", "TANHRE", "SQRE"]),
+    "forms_relu_linear": ("COS", "SECH", "GAUSS2", ["RELU", "LINEAR"]),
+}
+
+
+def potential_forms(name: str, seed: int = 4321) -> Potential:
+    cut, rform, aform, neurons = FORM_POTENTIALS[name]
+    nt = len(neurons)
+    return make_potential(nt, 6.0, 6, [4] * (nt * (nt + 1) // 2), [16, 16], seed, neuron=neurons, cut=cut,
+                          rform=rform, aform=aform)
 
 
 # --------------------------------------------------------------------------

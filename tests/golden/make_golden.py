@@ -50,6 +50,48 @@ def cases():
     return out
 
 
+def form_cases():
+    """(name, batch) of the fixtures of the other basis forms, cutoffs and
+    activations (synth.FORM_POTENTIALS): 4 periodic structures of 8-48 atoms."""
+    out = []
+    for n, name in enumerate(sorted(synth.FORM_POTENTIALS)):
+        nt = len(synth.FORM_POTENTIALS[name][3])
+        rng = np.random.default_rng(600 + n)
+        out.append((name, synth.batch_random(600 + n, rng.integers(8, 48, size=4), nt)))
+    return out
+
+
+def make_forms(name, b):
+    """A fixture of one FORM_POTENTIALS potential, conditioned on its own
+    batch's symmetry functions (the reference's), with the reference's
+    energies, forces and symmetry functions."""
+    import tempfile
+    pot = synth.potential_forms(name)
+    nt = pot.ntypes
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "pot.nnp")
+        potential.write(path, pot)
+        rp = ref.RefNNP(path)
+        G = np.concatenate([rp.compute(*b.structure(s), want_symm=True)[3] for s in range(b.n_struct)])
+        rp.close()
+        synth.condition(pot, G[:, :max(pot.n_input(t) for t in range(nt))], b.type)
+        potential.write(path, pot)
+        text = open(path).read()
+        rp = ref.RefNNP(path)
+        E, EV, F, Gs = [], [], [], []
+        for s in range(b.n_struct):
+            e, f, ev, g = rp.compute(*b.structure(s), want_symm=True)
+            E.append(e)
+            EV.append(ev)
+            F.append(f)
+            Gs.append(g)
+        rp.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), potential=np.frombuffer(text.encode(), dtype=np.uint8),
+                        atom_off=b.atom_off, pos=b.pos, type=b.type, cell=np.asarray(b.cell).reshape(-1, 9),
+                        pbc=np.array(True), energy=np.array(E), energy_vacuum=np.array(EV),
+                        forces=np.concatenate(F), symm=np.concatenate(Gs), config=np.array(0))
+
+
 def conditioning_batch(k):
     """Periodic structures of configuration k whose symmetry-function mean
     and spread set the network's input bias and scale (nnptefr's PREBIAS MEAN
@@ -191,6 +233,11 @@ if __name__ == "__main__":
         if which and name not in which:
             continue
         make(name, k, b, pbc)
+        print("wrote", name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
+    for name, b in form_cases():
+        if which and name not in which:
+            continue
+        make_forms(name, b)
         print("wrote", name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
     if not which or "train_config3" in which:
         make_train()

@@ -29,6 +29,7 @@ def load(path, tmp_path):
 def test_fixtures_present():
     names = {os.path.basename(p)[:-4] for p in GOLDEN}
     assert {"config1", "config2", "config3", "config4", "config5", "small_cells", "free_cluster"} <= names
+    assert set(synth.FORM_POTENTIALS) <= names
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
