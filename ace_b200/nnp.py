@@ -96,6 +96,7 @@ class NNP:
 
     def __init__(self, handle: C.c_void_p):
         self._h = handle
+        self.precision = PREC_FP32
 
     # ---- construction: NNP::read (nnp.cpp:181-190)
     @classmethod
@@ -170,6 +171,7 @@ class NNP:
 
     def set_precision(self, prec: int):
         self._check(lib().nnp_set_precision(self._h, prec))
+        self.precision = prec
 
     def set_loss(self, kind: int, delta: float = 1.0):
         """Energy-loss kind of train_grad (LOSS_MSE, LOSS_MAE, LOSS_HUBER,

@@ -399,6 +399,12 @@ def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
     t_max = float(t.item())
     all_atoms = float(atoms.item())
     value = all_atoms * args.steps / (t_max / 1e3)
+    # ---- the plain FP32 GPU path on the same batch and the same handle: the
+    # prebuilt generic kernels (no run-time specialisation), FP32 CUDA-core
+    # networks, eager launches (no CUDA graph); device-resident inputs, L2
+    # flushed, CUDA events, max over ranks, as for `value`
+    plain = time_plain(args, nn, subs, run_piece, flush, stream, world, dist, dev, all_atoms)
+
     # ---- stage times: a separate pass with the stage timers on (eager launches)
     nn.set_timing(True)
     stage_ms = {k: 0.0 for k in NNP.STAGES}
@@ -472,6 +478,7 @@ def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
                    "triplets_per_atom": round(fl["triplets"] / max(N, 1), 1),
                    "l2": "flushed before every timed call (256 MB write, not timed)",
                    "parallelism": "dp%d" % world},
+        "plain": dict(plain, ratio=round(value / plain["value"], 3)),
         "stage_ms": {k: round(v, 4) for k, v in per_step.items()},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -484,6 +491,43 @@ def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
                                     "p99": round(float(np.percentile(per_call, 99)), 4),
                                     "batches_per_step": len(subs), "structures_per_batch": STREAM_BATCH}
     return line, E_chk, F_chk
+
+
+def time_plain(args, nn, subs, run_piece, flush, stream, world, dist, dev, all_atoms):
+    """The plain FP32 GPU path: generic kernels, FP32 networks, no graph.
+    The handle's settings are restored afterwards."""
+    import torch
+    jit = bool(nn.specialization()[0])
+    prec = nn.precision
+    nn.set_specialization(False)
+    nn.set_precision(0)
+    nn.set_graphs(False)
+    for _ in range(args.warmup):
+        for k in range(len(subs)):
+            run_piece(k)
+    steps = max(1, min(args.steps, 10))
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in subs]
+          for _ in range(steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        for k in range(len(subs)):
+            flush.zero_()
+            ev[i][k][0].record(stream)
+            run_piece(k)
+            ev[i][k][1].record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([sum(a.elapsed_time(b_) for row in ev for a, b_ in row)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    nn.set_specialization(jit)
+    nn.set_precision(prec)
+    nn.set_graphs(True)
+    ms = float(t.item()) / steps
+    return {"value": round(all_atoms / (ms / 1e3), 1), "ms_per_step": round(ms, 4), "steps": steps,
+            "definition": "same batch and handle: prebuilt generic kernels, FP32 CUDA-core networks, eager "
+                          "launches (no CUDA graph)"}
 
 
 def add_cpu_baseline(line, name, nn, b, ppath, E_chk, F_chk):
