@@ -277,6 +277,9 @@ int finish_create(nnp_handle *h, nnp_handle **out)
     // the prebuilt kernels (a failed compilation does too, and is recorded)
     const char *env = std::getenv("NNP_JIT");
     E.use_jit = !(env && env[0] == '0');
+    nnp::tune_from_env(E.tune);
+    const char *at = std::getenv("NNP_AUTOTUNE");
+    E.autotune = at && at[0] == '1';
     if (E.use_jit) {
         E.jit_error = nnp::jit_build(E);
         if (!E.jit_error.empty()) E.use_jit = false;
@@ -499,6 +502,7 @@ int nnp_specialization_check(const char *potential_path, char *log, int32_t log_
     std::string src;
     std::vector<char> cubin;
     nnp::jit_last_log().clear();
+    nnp::tune_from_env(E.tune);
     msg = nnp::jit_compile(E, src, cubin);
     put(msg.empty() ? nnp::jit_last_log() + "\n" + src : msg);
     return msg.empty() ? NNP_OK : NNP_ERR_CUDA;
@@ -722,7 +726,7 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
                (int64_t)(intptr_t)E.pos.p, (int64_t)(intptr_t)E.type.p, (int64_t)(intptr_t)E.cell.p,
                (int64_t)(intptr_t)E.nbr.p, (int64_t)(intptr_t)E.G.p, (int64_t)(intptr_t)E.force.p,
                (int64_t)(intptr_t)E.e_struct.p, (int64_t)(intptr_t)E.e_atom.p, (int64_t)(intptr_t)E.vir.p};
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
         std::string msg;
         if (graphs && E.graph_exec && key == E.graph_key) {
             chk(cudaGraphLaunch((cudaGraphExec_t)E.graph_exec, E.stream));
@@ -785,6 +789,17 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
         }
         if (er.nonfinite == 2) { rc = fail(h, NNP_ERR_CUDA, "tensor-core network kernel: an MMA wait timed out"); break; }
         if (er.nonfinite) { rc = fail(h, NNP_ERR_NOT_FINITE, "non-finite energy or force"); }
+        // autotuning on and this capacity class not tuned yet: time the
+        // candidate kernels on this batch, then run the step again with the
+        // chosen ones (the class is marked tuned, so this happens once)
+        if (rc == NNP_OK && E.autotune && E.use_jit && E.jit_module && (flags & NNP_FORCES) &&
+            nnp::tune_needed(E, E.cap)) {
+            const std::string tm = nnp::autotune(E, E.cap, step);
+            E.graph_release();
+            graphs = false;
+            if (!tm.empty()) { rc = fail(h, NNP_ERR_CUDA, tm); break; }
+            continue;
+        }
         // outputs
         if (!devp) {
             const size_t be = sizeof(double) * S, bf = sizeof(double) * 3 * N;
@@ -963,6 +978,62 @@ int nnp_set_mma_wait(nnp_handle *h, int64_t polls)
     if (polls < 0 || polls > 0xffffffffll) return fail(h, NNP_ERR_ARG, "polls must be in [0, 2^32)");
     h->E.mma_wait_polls = (uint32_t)polls;
     h->E.graph_release();       // a captured step holds the old bound
+    return NNP_OK;
+}
+
+int nnp_set_autotune(nnp_handle *h, int32_t enable)
+{
+    if (!h) return NNP_ERR_ARG;
+    h->E.autotune = enable != 0;
+    return NNP_OK;
+}
+
+int nnp_tune_params(const nnp_handle *h, int32_t *params, int32_t n, int32_t *source, const char **log)
+{
+    if (!h || (n > 0 && !params) || n < 0) return NNP_ERR_ARG;
+    const nnp::TuneParams &p = h->E.tune;
+    const int32_t v[5] = {p.symm_minb, p.force_minb, p.force_unroll, p.force_chunk, p.tc_per_sm};
+    for (int k = 0; k < n && k < 5; ++k) params[k] = v[k];
+    if (source) *source = h->E.tune_source;
+    if (log) *log = h->E.tune_log.c_str();
+    return NNP_OK;
+}
+
+int nnp_tune_cache_key(const char *potential_path, const char *device_name, int32_t n_sm, int32_t cap, char *key,
+                       int32_t key_len)
+{
+    if (!potential_path || !device_name || !key || key_len <= 0 || n_sm <= 0 || cap <= 0) return NNP_ERR_ARG;
+    std::string text;
+    if (!read_file(potential_path, text)) return NNP_ERR_IO;
+    nnp::Engine E;
+    if (!nnp::read_potential(text, E.host).empty()) return NNP_ERR_PARSE;
+    if (!E.build_tables().empty()) return NNP_ERR_UNSUPPORTED;
+    const std::string k = nnp::tune_key(E, device_name, n_sm, cap);
+    if ((int32_t)k.size() + 1 > key_len) return NNP_ERR_CAPACITY;
+    std::memcpy(key, k.c_str(), k.size() + 1);
+    return NNP_OK;
+}
+
+int nnp_tune_cache_store(const char *key, const int32_t *params, int32_t n)
+{
+    if (!key || !params || n != 5) return NNP_ERR_ARG;
+    nnp::TuneParams p;
+    p.symm_minb = params[0];
+    p.force_minb = params[1];
+    p.force_unroll = params[2];
+    p.force_chunk = params[3];
+    p.tc_per_sm = params[4];
+    if (!nnp::tune_params_valid(p)) return NNP_ERR_ARG;
+    return nnp::tune_cache_store(key, p) ? NNP_OK : NNP_ERR_IO;
+}
+
+int nnp_tune_cache_load(const char *key, int32_t *params, int32_t n)
+{
+    if (!key || !params || n != 5) return NNP_ERR_ARG;
+    nnp::TuneParams p;
+    if (!nnp::tune_cache_load(key, p)) return NNP_ERR_IO;
+    const int32_t v[5] = {p.symm_minb, p.force_minb, p.force_unroll, p.force_chunk, p.tc_per_sm};
+    for (int k = 0; k < 5; ++k) params[k] = v[k];
     return NNP_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -46,6 +47,22 @@ struct DBuf {
     }
 };
 
+// Launch and tile choices of the per-atom kernels.  Defaults are the values
+// measured best on the batched workload; the autotuner (nnp_tune.cpp) times
+// alternatives on the caller's data and replaces them.
+struct TuneParams {
+    int symm_minb = 4;          // blocks per SM the specialised symmetry-function kernel's registers are budgeted for (1..4)
+    int force_minb = 1;         // the same for the specialised force kernel (1..4)
+    int force_unroll = 1;       // unroll factor of the specialised force kernel's pair loop (1..4)
+    int force_chunk = NNP_PCH;  // pairs per coefficient chunk of the force kernel (8..NNP_PCH)
+    int tc_per_sm = 0;          // CTAs per SM of the tensor-core network kernel (0: as many as fit, at most 4)
+    bool operator==(const TuneParams &o) const
+    {
+        return symm_minb == o.symm_minb && force_minb == o.force_minb && force_unroll == o.force_unroll &&
+               force_chunk == o.force_chunk && tc_per_sm == o.tc_per_sm;
+    }
+};
+
 struct Engine {
     // potential
     HostPot host;
@@ -66,6 +83,11 @@ struct Engine {
     std::vector<double> vac_host;
 
     // kernels specialised for this potential at run time (nnp_jit.cpp)
+    TuneParams tune;              // launch / tile choices the specialised kernels are compiled with
+    bool autotune = false;        // tune on the first call of each neighbour-capacity class (nnp_set_autotune)
+    std::vector<int> tuned_caps;  // capacity classes already tuned (or loaded from the cache) by this handle
+    int tune_source = 0;          // 0 defaults, 1 loaded from the tuning cache, 2 tuned on this handle's data
+    std::string tune_log;         // the last tuning's measurements
     bool use_jit = true;
     void *jit_module = nullptr;   // cudaLibrary_t
     void *jit_symm = nullptr, *jit_force = nullptr, *jit_tangent = nullptr;   // cudaKernel_t
@@ -151,8 +173,22 @@ std::string run_nn_tc(Engine &E, bool split);
 std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,
                                     const float *G, int gstride, bool vacuum, double *energy);
 
+// autotuner (nnp_tune.cpp): key of the tuning cache and the tuning itself,
+// which calls run_step (the device-side step, stage timers on) per candidate
+std::string tune_key(const Engine &E, const std::string &device, int nsm, int cap);
+bool tune_cache_load(const std::string &key, TuneParams &p);
+bool tune_cache_store(const std::string &key, const TuneParams &p);
+std::string autotune(Engine &E, int cap, const std::function<std::string()> &run_step);
+bool tune_needed(const Engine &E, int cap);
+bool tune_params_valid(const TuneParams &p);
+void tune_from_env(TuneParams &p);
+
 // run-time specialised kernels (nnp_jit.cpp)
 std::string jit_compile(const Engine &E, std::string &source, std::vector<char> &cubin);
+std::string jit_compile_params(const Engine &E, const TuneParams &tp, std::string &source, std::vector<char> &cubin);
+std::string jit_source(const Engine &E, const TuneParams &p);
+uint64_t source_hash(const std::string &s);
+std::string cache_dir();
 std::string jit_build(Engine &E);
 std::string &jit_last_log();   // compiler messages of the last NVRTC compilation
 void jit_release(Engine &E);

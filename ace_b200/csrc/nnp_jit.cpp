@@ -356,31 +356,22 @@ std::string group_cases(const std::vector<std::pair<int, std::string>> &cases)
     return os.str();
 }
 
-std::string make_source(const Engine &E)
+std::string make_source(const Engine &E, const TuneParams &tp)
 {
     std::ostringstream os;
-    // Launch-bound and unroll choices, as macros at the top of the source.
-    // Resident blocks per SM the compiler budgets registers for (at most 255,
-    // 128, 85, 64 registers for 1..4 blocks of NNP_WARPS warps).  Measured on
-    // the batched workload: 4 blocks make the symmetry-function kernel 3 %
-    // faster than 3 (64 instead of 71 registers; its shared memory allows 4);
-    // the force kernel is fastest unconstrained (115 registers, 2 blocks by
-    // its shared memory; capped at 128 registers it is 3 % slower).
-    // NNP_SYMM_MINB / NNP_FORCE_MINB / NNP_FORCE_UNROLL override the defaults
-    // (1 .. 4).
-    auto knob = [](const char *name, int def) {
-        const char *v = std::getenv(name);
-        const int b = (v && v[0]) ? std::atoi(v) : def;
-        return (b >= 1 && b <= 4) ? b : def;
-    };
-    os << "#define NNP_SYMM_MINB " << knob("NNP_SYMM_MINB", 4) << "\n#define NNP_FORCE_MINB "
-       << knob("NNP_FORCE_MINB", 1) << "\n#define NNP_FORCE_UNROLL " << knob("NNP_FORCE_UNROLL", 1) << "\n";
-    // NNP_FORCE_CHUNK (1 .. NNP_PCH): pairs per chunk of the force kernel;
-    // small values split the pair rows between many chunks (used by a test)
-    if (const char *c = std::getenv("NNP_FORCE_CHUNK")) {
-        const int n = std::atoi(c);
-        if (n >= 1 && n <= NNP_PCH) os << "#define NNP_FORCE_CHUNK " << n << "\n";
-    }
+    // Launch-bound, unroll and chunk choices, as macros at the top of the
+    // source (TuneParams; defaults in nnp_engine.h, replaced by the
+    // autotuner).  Resident blocks per SM the compiler budgets registers for
+    // (at most 255, 128, 85, 64 registers for 1..4 blocks of NNP_WARPS warps).
+    // Measured on the batched workload: 4 blocks make the symmetry-function
+    // kernel 3 % faster than 3 (64 instead of 71 registers; its shared memory
+    // allows 4); the force kernel is fastest unconstrained (115 registers, 2
+    // blocks by its shared memory; capped at 128 registers it is 3 % slower).
+    os << "#define NNP_SYMM_MINB " << tp.symm_minb << "\n#define NNP_FORCE_MINB " << tp.force_minb
+       << "\n#define NNP_FORCE_UNROLL " << tp.force_unroll << "\n";
+    // pairs per chunk of the force kernel; small values split the pair rows
+    // between many chunks (used by a test)
+    if (tp.force_chunk != NNP_PCH) os << "#define NNP_FORCE_CHUNK " << tp.force_chunk << "\n";
     os << "#include \"nnp_device.cuh\"\nnamespace nnp {\nstruct JitBlocks {\n";
     std::vector<std::pair<int, std::string>> sy, fo, ta, ra;
     const int T = E.dpot.ntypes, TT = T * (T + 1) / 2;
@@ -452,6 +443,8 @@ k_tangent_jit(long long N, const nnp::DevPot *__restrict__ pot, const float2 *__
 
 }  // namespace
 
+std::string jit_source(const Engine &E, const TuneParams &p) { return make_source(E, p); }
+
 void jit_release(Engine &E)
 {
     if (E.jit_module) cudaLibraryUnload((cudaLibrary_t)E.jit_module);
@@ -465,7 +458,7 @@ std::string &jit_last_log()
     return log;
 }
 
-// 64-bit FNV-1a of the source: key of the compiled-kernel caches
+// 64-bit FNV-1a of a text: key of the compiled-kernel and tuning caches
 uint64_t source_hash(const std::string &s)
 {
     uint64_t h = 1469598103934665603ull;
@@ -476,25 +469,39 @@ uint64_t source_hash(const std::string &s)
     return h;
 }
 
-std::string cache_path(uint64_t h)
+// Directory of the on-disk caches: NNP_CACHE_DIR, else ~/.cache/nnp_b200
+// ("" when neither is known).
+std::string cache_dir()
 {
     const char *dir = std::getenv("NNP_CACHE_DIR");
-    std::string d;
-    if (dir && dir[0]) d = dir;
-    else if (const char *home = std::getenv("HOME")) d = std::string(home) + "/.cache/nnp_b200";
-    else return "";
+    if (dir && dir[0]) return dir;
+    if (const char *home = std::getenv("HOME")) return std::string(home) + "/.cache/nnp_b200";
+    return "";
+}
+
+std::string cache_path(uint64_t h)
+{
+    const std::string d = cache_dir();
+    if (d.empty()) return "";
     char name[64];
     std::snprintf(name, sizeof name, "/%016llx.cubin", (unsigned long long)h);
     return d + name;
 }
 
-// Compiles the specialised kernels; cubins are kept per process and on disk
-// (NNP_CACHE_DIR, default ~/.cache/nnp_b200) by a hash of the source.
+// Compiles the specialised kernels with the handle's launch choices.
 std::string jit_compile(const Engine &E, std::string &source, std::vector<char> &cubin)
+{
+    return jit_compile_params(E, E.tune, source, cubin);
+}
+
+// Compiles the specialised kernels with launch choices tp; cubins are kept
+// per process and on disk (cache_dir()) by a hash of the source.  Safe to call
+// from several host threads at once.
+std::string jit_compile_params(const Engine &E, const TuneParams &tp, std::string &source, std::vector<char> &cubin)
 {
     static std::mutex mu;
     static std::map<uint64_t, std::vector<char>> memo;
-    source = make_source(E);
+    source = make_source(E, tp);
     const uint64_t key = source_hash(source + kDeviceHeaderSource);
     {
         std::lock_guard<std::mutex> lk(mu);

@@ -480,7 +480,8 @@ std::string run_nn_tc(Engine &E, bool split)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // at most 4 CTAs per SM: 4 x 128 TMEM columns is the SM's 512
-    const int per_sm = std::max(1, std::min(4, (228 * 1024) / (sm + 1024)));
+    int per_sm = std::max(1, std::min(4, (228 * 1024) / (sm + 1024)));
+    if (E.tune.tc_per_sm > 0) per_sm = std::min(per_sm, E.tune.tc_per_sm);   // autotuned (nnp_tune.cpp)
     const int64_t tiles = (N + TILE - 1) / TILE + E.dpot.ntypes;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)nsm * per_sm));
     const uint32_t polls = E.mma_wait_polls > 0 ? E.mma_wait_polls : WAIT_POLLS;

@@ -69,6 +69,11 @@ def lib():
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
             "nnp_set_loss": ([p, i, d], i),
             "nnp_set_mma_wait": ([p, C.c_int64], i),
+            "nnp_set_autotune": ([p, i], i),
+            "nnp_tune_params": ([p, p, i, C.POINTER(i), C.POINTER(C.c_char_p)], i),
+            "nnp_tune_cache_key": ([C.c_char_p, C.c_char_p, i, i, C.c_char_p, i], i),
+            "nnp_tune_cache_store": ([C.c_char_p, p, i], i),
+            "nnp_tune_cache_load": ([C.c_char_p, p, i], i),
             "nnp_set_accumulation": ([p, i], i),
             "nnp_set_specialization": ([p, i], i),
             "nnp_specialization": ([p, C.POINTER(i), C.POINTER(C.c_char_p)], i),
@@ -181,6 +186,22 @@ class NNP:
     def set_mma_wait(self, polls: int):
         """Bound of each tensor-core MMA-chain wait (0: the default)."""
         self._check(lib().nnp_set_mma_wait(self._h, int(polls)))
+
+    def set_autotune(self, on: bool = True):
+        """Tune the kernels' launch and tile choices on the first energy+force
+        call of each neighbour-capacity class (cached on disk)."""
+        self._check(lib().nnp_set_autotune(self._h, 1 if on else 0))
+
+    TUNE_NAMES = ("symm_minb", "force_minb", "force_unroll", "force_chunk", "tc_per_sm")
+
+    def tune_params(self):
+        """(choices as a dict, source: "default" | "cache" | "tuned", log)."""
+        v = np.zeros(5, dtype=np.int32)
+        src = C.c_int32()
+        log = C.c_char_p()
+        self._check(lib().nnp_tune_params(self._h, _ptr(v), 5, C.byref(src), C.byref(log)))
+        return (dict(zip(self.TUNE_NAMES, (int(x) for x in v))), ("default", "cache", "tuned")[src.value],
+                (log.value or b"").decode())
 
     def set_graphs(self, on: bool = True):
         """Replay the device-side step as a CUDA graph while calls repeat their shape."""
@@ -338,3 +359,26 @@ class NNP:
         self._check(lib().nnp_train_grad(self._h, C.byref(b), _ptr(e_ref), _ptr(f_ref), float(w_f), norm_mode,
                                          _ptr(loss), _ptr(g), _ptr(eo), _ptr(fo), 0))
         return float(loss[0]), g, eo, fo
+
+
+def tune_cache_key(potential_path: str, device_name: str, n_sm: int, cap: int) -> str:
+    """Key of the tuning cache for a potential on a GPU model and capacity (no GPU needed)."""
+    buf = C.create_string_buffer(256)
+    rc = lib().nnp_tune_cache_key(os.fsencode(potential_path), device_name.encode(), n_sm, cap, buf, len(buf))
+    if rc != NNP_OK:
+        raise NNPError(rc, "tune_cache_key failed")
+    return buf.value.decode()
+
+
+def tune_cache_store(key: str, params: dict) -> None:
+    v = np.array([params[k] for k in NNP.TUNE_NAMES], dtype=np.int32)
+    rc = lib().nnp_tune_cache_store(key.encode(), _ptr(v), 5)
+    if rc != NNP_OK:
+        raise NNPError(rc, "tune_cache_store failed")
+
+
+def tune_cache_load(key: str):
+    """The stored choices of key as a dict, or None."""
+    v = np.zeros(5, dtype=np.int32)
+    rc = lib().nnp_tune_cache_load(key.encode(), _ptr(v), 5)
+    return None if rc != NNP_OK else dict(zip(NNP.TUNE_NAMES, (int(x) for x in v)))

@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16", "bf16x3"],
                     help="network layers: FP32 CUDA cores, or BF16 / split-BF16 tensor cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch and tile choices")
     return ap.parse_args()
 
 
@@ -321,6 +322,8 @@ def main():
     pot = build_potential(name, ppath)
     nn = NNP.read(ppath)
     nn.set_precision(PRECISION[args.precision])
+    # launch and tile choices tuned on the first call of this batch (cached on disk)
+    nn.set_autotune(not args.no_autotune)
     # a stream of our own: the library can capture and replay its step as a
     # CUDA graph on it (not on the legacy default stream)
     stream = torch.cuda.Stream(dev)
@@ -485,12 +488,19 @@ def time_inference(args, name, nn, pot, b, world, dist, clocks, dev, stream):
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "tuning": tuning_summary(nn),
     }
     if name == "stream":
         line["batch_latency_ms"] = {"p50": round(float(np.percentile(per_call, 50)), 4),
                                     "p99": round(float(np.percentile(per_call, 99)), 4),
                                     "batches_per_step": len(subs), "structures_per_batch": STREAM_BATCH}
     return line, E_chk, F_chk
+
+
+def tuning_summary(nn):
+    """The kernels' launch and tile choices and where they came from."""
+    choices, source, log = nn.tune_params()
+    return {"choices": choices, "source": source, "log": log}
 
 
 def time_plain(args, nn, subs, run_piece, flush, stream, world, dist, dev, all_atoms):

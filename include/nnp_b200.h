@@ -121,6 +121,33 @@ int nnp_specialization(const nnp_handle *h, int32_t *active, const char **source
  * when compilation fails (NNP_ERR_CUDA). */
 int nnp_specialization_check(const char *potential_path, char *log, int32_t log_len);
 
+/* Autotuning of the launch and tile choices of the per-atom kernels (no
+ * reference counterpart; the reference runs on the CPU).  With enable = 1
+ * (or NNP_AUTOTUNE=1 in the environment at creation), the first
+ * energy+force call of each neighbour-capacity class (64, 128, 256 slots per
+ * atom) looks the choice up in the tuning cache (NNP_CACHE_DIR, default
+ * ~/.cache/nnp_b200, file tuning.txt), keyed by the potential, the network
+ * shapes, the precision, the GPU and the class; without an entry it compiles
+ * a few candidates and times each on that call's own batch (CUDA events),
+ * keeps the fastest choice of each kernel, stores it, and then computes the
+ * call's results with it.  The first such call therefore takes seconds
+ * longer.  Results do not depend on the choices beyond FP32 summation order.
+ * Choices (params[0..4]): blocks per SM the symmetry-function kernel's
+ * registers are budgeted for, the same for the force kernel, the force
+ * kernel's pair-loop unroll, its pairs per coefficient chunk, and CTAs per
+ * SM of the tensor-core network kernel (0 = as many as fit).
+ * nnp_tune_params returns the handle's current choices, where they came from
+ * (*source: 0 defaults, 1 tuning cache, 2 tuned on this handle) and the last
+ * tuning's measurements (*log).  nnp_tune_cache_key / _store / _load read and
+ * write the cache without a GPU (e.g. to seed it for a fleet of one GPU model):
+ * key has room for key_len bytes (about 100 are needed). */
+int nnp_set_autotune(nnp_handle *h, int32_t enable);
+int nnp_tune_params(const nnp_handle *h, int32_t *params, int32_t n, int32_t *source, const char **log);
+int nnp_tune_cache_key(const char *potential_path, const char *device_name, int32_t n_sm, int32_t cap, char *key,
+                       int32_t key_len);
+int nnp_tune_cache_store(const char *key, const int32_t *params, int32_t n);
+int nnp_tune_cache_load(const char *key, int32_t *params, int32_t n);
+
 /* Launch on this CUDA stream (cudaStream_t) instead of the handle's own one. */
 int nnp_set_stream(nnp_handle *h, void *cuda_stream);
 
