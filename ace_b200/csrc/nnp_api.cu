@@ -62,8 +62,9 @@ namespace nnp {
 void Engine::free_all()
 {
     rpar.release(); apar.release(); wpar.release(); vac.release();
+    rpar64.release(); apar64.release(); cut64.release();
     atom_off.release(); pos.release(); cell.release(); xw.release();
-    type.release(); atom_struct.release(); atom_cell.release(); grid.release();
+    type.release(); atom_struct.release(); atom_cell.release(); grid.release(); bbox.release();
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
     cell_tcnt.release();
     cell_pos.release(); order.release(); type_fill.release();
@@ -117,6 +118,8 @@ std::string Engine::build_tables()
     };
     std::vector<float2> rp;
     std::vector<float4> ap;
+    std::vector<double2> rp64;
+    std::vector<double4> ap64;
     std::vector<float> wp;
     std::vector<double> vc(T);
     for (int II = 0; II < T; ++II) {
@@ -131,7 +134,10 @@ std::string Engine::build_tables()
             const int c = cut_id(b.cut, b.rc);
             if (c < 0) return "too many distinct cutoffs in the potential";
             t.br[J] = {n, off, b.form, c, (int)rp.size()};
-            for (int f = 0; f < n; ++f) rp.push_back(make_float2((float)b.rs[f], (float)b.eta[f]));
+            for (int f = 0; f < n; ++f) {
+                rp.push_back(make_float2((float)b.rs[f], (float)b.eta[f]));
+                rp64.push_back(make_double2(b.rs[f], b.eta[f]));
+            }
             off += n;
         }
         int offa = t.n_input_r;
@@ -167,6 +173,7 @@ std::string Engine::build_tables()
                 float w;
                 std::memcpy(&w, &pk, sizeof w);
                 ap.push_back(make_float4((float)(0.5 * b.lambda[f]), (float)z, (float)a, w));
+                ap64.push_back(make_double4(0.5 * b.lambda[f], z, a, 0.0));
             }
             t.ba[tt] = {n, offa, b.form, c, (int)ap.size() - n, int_zeta};
             offa += n;
@@ -209,6 +216,10 @@ std::string Engine::build_tables()
     wfloats = (int64_t)wp.size();
     rpar_host = rp;
     apar_host = ap;
+    rpar64_host = rp64;
+    apar64_host = ap64;
+    cut64_host.clear();
+    for (const auto &c : cuts) cut64_host.push_back(c.second);
     wpar_host = wp;
     vac_host = vc;
     dpot = d;
@@ -226,6 +237,12 @@ std::string Engine::upload()
     const std::vector<double> &vc = vac_host;
     if (rp.empty()) rp.push_back(make_float2(0.f, 0.f));
     if (ap.empty()) ap.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<double2> rp64 = rpar64_host;
+    std::vector<double4> ap64 = apar64_host;
+    std::vector<double> c64 = cut64_host;
+    if (rp64.empty()) rp64.push_back(make_double2(0.0, 0.0));
+    if (ap64.empty()) ap64.push_back(make_double4(0.0, 0.0, 0.0, 0.0));
+    if (c64.empty()) c64.push_back(0.0);
     cudaError_t e = cudaSuccess;
     auto r = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
     if (!d_pot) r(cudaMalloc((void **)&d_pot, sizeof(DevPot)));
@@ -233,12 +250,18 @@ std::string Engine::upload()
     r(apar.reserve(ap.size()));
     r(wpar.reserve(wp.size()));
     r(vac.reserve(vc.size()));
+    r(rpar64.reserve(rp64.size()));
+    r(apar64.reserve(ap64.size()));
+    r(cut64.reserve(c64.size()));
     if (e != cudaSuccess) return std::string("device allocation failed: ") + cudaGetErrorString(e);
     r(cudaMemcpy(d_pot, &d, sizeof d, cudaMemcpyHostToDevice));
     r(cudaMemcpy(rpar.p, rp.data(), rp.size() * sizeof(float2), cudaMemcpyHostToDevice));
     r(cudaMemcpy(apar.p, ap.data(), ap.size() * sizeof(float4), cudaMemcpyHostToDevice));
     r(cudaMemcpy(wpar.p, wp.data(), wp.size() * sizeof(float), cudaMemcpyHostToDevice));
     r(cudaMemcpy(vac.p, vc.data(), vc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(rpar64.p, rp64.data(), rp64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(apar64.p, ap64.data(), ap64.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    r(cudaMemcpy(cut64.p, c64.data(), c64.size() * sizeof(double), cudaMemcpyHostToDevice));
     if (e != cudaSuccess) return std::string("potential upload failed: ") + cudaGetErrorString(e);
     return "";
 }
@@ -313,7 +336,7 @@ cudaError_t h2d(nnp::Engine &E, void *dst, const void *src, size_t bytes, size_t
     return cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, E.stream);
 }
 
-int estimate_cap(const nnp_batch *b, double rc)
+int estimate_cap(const nnp_batch *b, double rc, int64_t n_ghost)
 {
     double pmax = 16.0;
     for (int s = 0; s < b->n_struct; ++s) {
@@ -325,6 +348,18 @@ int estimate_cap(const nnp_batch *b, double rc)
             const double V = std::fabs(c[0] * (c[4] * c[8] - c[5] * c[7]) - c[1] * (c[3] * c[8] - c[5] * c[6]) +
                                        c[2] * (c[3] * c[7] - c[4] * c[6]));
             p = V > 0 ? 4.18879020478639 * rc * rc * rc * (double)n / V : 256.0;
+        } else if (n_ghost > 0) {
+            // local + ghost atoms: the density of the local atoms' bounding box
+            const int64_t a0 = b->atom_off[s], nl = std::max<int64_t>(n - n_ghost, 1);
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int64_t a = a0; a < a0 + nl; ++a)
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = std::min(lo[d], b->pos[3 * a + d]);
+                    hi[d] = std::max(hi[d], b->pos[3 * a + d]);
+                }
+            double V = 1.0;
+            for (int d = 0; d < 3; ++d) V *= std::max(hi[d] - lo[d], rc);
+            p = std::min(4.18879020478639 * rc * rc * rc * (double)nl / V, (double)(n - 1));
         } else {
             p = (double)(n - 1);
         }
@@ -519,8 +554,10 @@ int nnp_set_graphs(nnp_handle *h, int32_t enable)
 int nnp_set_accumulation(nnp_handle *h, int32_t acc)
 {
     if (!h) return NNP_ERR_ARG;
-    if (acc != NNP_ACC_FP32 && acc != NNP_ACC_FP64) return fail(h, NNP_ERR_ARG, "unknown accumulation mode");
+    if (acc != NNP_ACC_FP32 && acc != NNP_ACC_FP64 && acc != NNP_SYMM_FP64)
+        return fail(h, NNP_ERR_ARG, "unknown accumulation mode");
     h->E.acc64 = (acc == NNP_ACC_FP64);
+    h->E.symm64 = (acc == NNP_SYMM_FP64);
     return NNP_OK;
 }
 
@@ -628,10 +665,11 @@ namespace {
 // nnp_compute and nnp_compute_md: the whole pipeline, with the optional
 // per-atom energies [N] and per-structure virials [9 S] of the MD call.
 int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out,
-                 double *atom_energy, double *virial, uint32_t flags)
+                 double *atom_energy, double *virial, uint32_t flags, int64_t n_ghost = 0)
 {
     if (!h || !b) return NNP_ERR_ARG;
     nnp::Engine &E = h->E;
+    E.n_ghost = n_ghost;
     if (b->n_struct < 0) return fail(h, NNP_ERR_ARG, "negative structure count");
     if ((flags & NNP_ENERGY) && !energy) return fail(h, NNP_ERR_ARG, "energy output missing");
     if ((flags & NNP_FORCES) && !forces) return fail(h, NNP_ERR_ARG, "force output missing");
@@ -657,7 +695,7 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
             for (int64_t i = 0; i < N; ++i)
                 if (b->type[i] < 0 || b->type[i] >= T)
                     return fail(h, NNP_ERR_TYPE, "atom " + std::to_string(i) + " has type index " + std::to_string(b->type[i]) + " outside [0," + std::to_string(T) + ")");
-        E.cap = std::max(E.cap, estimate_cap(b, E.host.rc));
+        E.cap = std::max(E.cap, estimate_cap(b, E.host.rc, n_ghost));
         // inputs -> device
         const size_t bo = sizeof(int64_t) * (S + 1), bp = sizeof(double) * 3 * N, bt = sizeof(int32_t) * N,
                      bc = b->pbc ? sizeof(double) * 9 * S : 0;
@@ -720,8 +758,8 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
                   E.stream != cudaStreamPerThread;
     std::vector<int64_t> key;
     if (graphs)
-        key = {N, S, b->pbc, E.cap, (int64_t)flags, (int64_t)(atom_energy != nullptr), (int64_t)(virial != nullptr),
-               E.precision, (int64_t)(intptr_t)(E.use_jit ? E.jit_symm : nullptr), (int64_t)E.acc64,
+        key = {N, S, b->pbc, n_ghost, E.cap, (int64_t)flags, (int64_t)(atom_energy != nullptr), (int64_t)(virial != nullptr),
+               E.precision, (int64_t)(intptr_t)(E.use_jit ? E.jit_symm : nullptr), (int64_t)E.acc64 + 2 * E.symm64,
                (int64_t)(intptr_t)E.atom_off.p,
                (int64_t)(intptr_t)E.pos.p, (int64_t)(intptr_t)E.type.p, (int64_t)(intptr_t)E.cell.p,
                (int64_t)(intptr_t)E.nbr.p, (int64_t)(intptr_t)E.G.p, (int64_t)(intptr_t)E.force.p,
@@ -812,7 +850,8 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
             }
             if (atom_energy) {
                 nnp::run_atom_energy(E, (flags & NNP_VACUUM) != 0, E.eatom_d.p);
-                chk(cudaMemcpyAsync(atom_energy, E.eatom_d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, E.stream));
+                chk(cudaMemcpyAsync(atom_energy, E.eatom_d.p, sizeof(double) * (N - n_ghost), cudaMemcpyDeviceToHost,
+                                    E.stream));
             }
             if (virial) chk(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost, E.stream));
         } else {
@@ -853,6 +892,27 @@ int nnp_compute_md(nnp_handle *h, const nnp_batch *b, double *energy, double *fo
     if (!energy && !forces && !atom_energy && !virial) return fail(h, NNP_ERR_ARG, "no output requested");
     flags |= (energy ? NNP_ENERGY : 0u) | (forces ? NNP_FORCES : 0u);
     return compute_impl(h, b, energy, forces, nullptr, atom_energy, virial, flags);
+}
+
+int nnp_compute_local_ghost(nnp_handle *h, int64_t n_local, int64_t n_ghost, const double *pos,
+                            const int32_t *type, double *energy, double *forces, double *atom_energy, double *virial,
+                            uint32_t flags)
+{
+    if (!h) return NNP_ERR_ARG;
+    if (flags & ~(uint32_t)NNP_VACUUM) return fail(h, NNP_ERR_ARG, "flags other than NNP_VACUUM");
+    if (n_local < 0 || n_ghost < 0) return fail(h, NNP_ERR_ARG, "negative atom count");
+    if (!energy && !forces && !atom_energy && !virial) return fail(h, NNP_ERR_ARG, "no output requested");
+    if (n_local + n_ghost == 0) {
+        if (energy) *energy = 0.0;
+        if (virial)
+            for (int k = 0; k < 9; ++k) virial[k] = 0.0;
+        return NNP_OK;
+    }
+    if (!pos || !type) return fail(h, NNP_ERR_ARG, "positions and types are required");
+    const int64_t off[2] = {0, n_local + n_ghost};
+    const nnp_batch b = {1, off, pos, type, nullptr, 0};
+    flags |= (energy ? NNP_ENERGY : 0u) | (forces ? NNP_FORCES : 0u);
+    return compute_impl(h, &b, energy, forces, nullptr, atom_energy, virial, flags, n_ghost);
 }
 
 int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, const int64_t *d_atom_off,

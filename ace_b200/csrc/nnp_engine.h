@@ -77,6 +77,13 @@ struct Engine {
     int precision = 0;
     uint32_t mma_wait_polls = 0;  // bound of one tensor-core MMA-chain wait (0: the kernel's default)
     bool acc64 = false;           // FP64 running sums of the symmetry functions
+    bool symm64 = false;          // symmetry functions evaluated in FP64 (k_symm_f64)
+    DBuf<double2> rpar64;         // radial (rs, eta) in FP64
+    DBuf<double4> apar64;         // angular (lambda/2, zeta, 1/eta_run^2, 0) in FP64
+    DBuf<double> cut64;           // rc of every distinct cutoff in FP64
+    std::vector<double2> rpar64_host;
+    std::vector<double4> apar64_host;
+    std::vector<double> cut64_host;
     std::vector<float2> rpar_host;
     std::vector<float4> apar_host;
     std::vector<float> wpar_host;
@@ -100,12 +107,15 @@ struct Engine {
     // batch
     int n_struct = 0;
     int64_t n_atoms = 0;
+    int64_t n_ghost = 0;          // the last n_ghost atoms are ghosts: neighbours only (nnp_compute_local_ghost)
+    int64_t n_centre = 0;         // n_atoms - n_ghost: atoms that are centres (own an energy and symmetry functions)
     int cap = 0;                  // neighbour slots per atom
     int tot_cells = 0;
     DBuf<int64_t> atom_off;
     DBuf<double> pos, cell, xw;
     DBuf<int> type, atom_struct, atom_cell;
     DBuf<StructGrid> grid;
+    DBuf<double> bbox;            // bounding box of each free structure [6 * S]
     DBuf<int> cell_cnt, cell_start, cell_fill, cell_atoms, scan_tmp;
     DBuf<int> cell_tcnt;          // members of each type per cell [cell][type]
     DBuf<double4> cell_pos;       // cell-ordered wrapped positions, type in .w

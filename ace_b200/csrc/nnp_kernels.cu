@@ -70,7 +70,10 @@ __global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N,
 // atomic per (block, element) to count, then one to reserve each block's range.
 // Atoms whose type is outside [0, ntypes) go last, in slot ntypes (the kernels
 // that walk the order skip them; the call reports the bad type).
-__global__ void k_type_count(int64_t N, const int *__restrict__ type, int ntypes, int *__restrict__ cnt)
+// Atoms [n_centre, N) are ghosts (neighbours only, never centres): they are
+// counted with the out-of-range types, so `order` lists them last.
+__global__ void k_type_count(int64_t N, int64_t n_centre, const int *__restrict__ type, int ntypes,
+                             int *__restrict__ cnt)
 {
     __shared__ int c[NNP_MAX_TYPES + 1];
     if (threadIdx.x <= NNP_MAX_TYPES) c[threadIdx.x] = 0;
@@ -78,14 +81,14 @@ __global__ void k_type_count(int64_t N, const int *__restrict__ type, int ntypes
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < N) {
         const int t = type[i];
-        atomicAdd(&c[(t >= 0 && t < ntypes) ? t : ntypes], 1);
+        atomicAdd(&c[(t >= 0 && t < ntypes && i < n_centre) ? t : ntypes], 1);
     }
     __syncthreads();
     if (threadIdx.x <= ntypes && c[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], c[threadIdx.x]);
 }
 
-__global__ void k_type_scatter(int64_t N, const int *__restrict__ type, int ntypes, const int *__restrict__ cnt,
-                               int *__restrict__ fill, int *__restrict__ order)
+__global__ void k_type_scatter(int64_t N, int64_t n_centre, const int *__restrict__ type, int ntypes,
+                               const int *__restrict__ cnt, int *__restrict__ fill, int *__restrict__ order)
 {
     __shared__ int c[NNP_MAX_TYPES + 1], base[NNP_MAX_TYPES + 1];
     if (threadIdx.x <= NNP_MAX_TYPES) c[threadIdx.x] = 0;
@@ -94,7 +97,7 @@ __global__ void k_type_scatter(int64_t N, const int *__restrict__ type, int ntyp
     int t = -1, r = 0;
     if (i < N) {
         t = type[i];
-        if (!(t >= 0 && t < ntypes)) t = ntypes;
+        if (!(t >= 0 && t < ntypes) || i >= n_centre) t = ntypes;
         r = atomicAdd(&c[t], 1);
     }
     __syncthreads();
@@ -107,8 +110,42 @@ __global__ void k_type_scatter(int64_t N, const int *__restrict__ type, int ntyp
     if (t >= 0) order[base[t] + r] = (int)i;
 }
 
+// Bounding box of every structure (free boundaries only): bbox[6s..6s+2] the
+// smallest, bbox[6s+3..6s+5] the largest coordinate.  One block per structure.
+__global__ void k_struct_bbox(const double *__restrict__ pos, const int64_t *__restrict__ off,
+                              double *__restrict__ bbox)
+{
+    __shared__ double lo[3][256], hi[3][256];
+    const int s = blockIdx.x, t = threadIdx.x;
+    double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
+    for (int64_t a = off[s] + t; a < off[s + 1]; a += blockDim.x)
+        for (int d = 0; d < 3; ++d) {
+            const double x = pos[3 * a + d];
+            l[d] = fmin(l[d], x);
+            h[d] = fmax(h[d], x);
+        }
+    for (int d = 0; d < 3; ++d) { lo[d][t] = l[d]; hi[d][t] = h[d]; }
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if (t < k)
+            for (int d = 0; d < 3; ++d) {
+                lo[d][t] = fmin(lo[d][t], lo[d][t + k]);
+                hi[d][t] = fmax(hi[d][t], hi[d][t + k]);
+            }
+        __syncthreads();
+    }
+    if (t == 0)
+        for (int d = 0; d < 3; ++d) { bbox[6 * s + d] = lo[d][0]; bbox[6 * s + 3 + d] = hi[d][0]; }
+}
+
+// A free structure of more than this many atoms is searched through a cell
+// grid over its bounding box (smaller ones are one cell, every atom a
+// candidate of every other).
+#define NNP_FREE_ONE_CELL 2048
+
 __global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *__restrict__ off, int S, int pbc,
-                               double rc, StructGrid *__restrict__ grid, int *__restrict__ ncells, DevErr *err)
+                               double rc, const double *__restrict__ bbox, StructGrid *__restrict__ grid,
+                               int *__restrict__ ncells, DevErr *err)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -119,8 +156,18 @@ __global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *_
     g.m[0] = g.m[1] = g.m[2] = 0;
     g.pbc = pbc;
     g.cell_base = 0;
-    if (pbc) {
-        for (int k = 0; k < 9; ++k) g.R[k] = cell[9 * (int64_t)s + k];
+    // A large free structure is put in an orthorhombic periodic box at least
+    // rc (+1 A) wider than its bounding box in every direction, so no periodic
+    // image of an atom comes within rc of another: the cell-list search of the
+    // periodic path then finds exactly the free structure's neighbours.
+    const bool boxed = !pbc && nat > NNP_FREE_ONE_CELL;
+    if (boxed) {
+        for (int d = 0; d < 3; ++d) g.R[4 * d] = (bbox[6 * s + 3 + d] - bbox[6 * s + d]) + rc + 1.0;
+        g.pbc = 1;
+    }
+    if (pbc || boxed) {
+        if (pbc)
+            for (int k = 0; k < 9; ++k) g.R[k] = cell[9 * (int64_t)s + k];
         const double *a[3] = {g.R, g.R + 3, g.R + 6};
         double c[3][3];
         for (int n = 0; n < 3; ++n) {
@@ -660,6 +707,197 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_symm(int64_t N, const DevPot 
 
 // One warp per atom: forward pass, atomic energy, and the input gradient
 // dE/dG = outw d_L W_L ... d_0 W_0 diag(inpw) (DODZ::grad).
+// ------------------------------------------------------------------ FP64 symmetry functions
+#define NNP_PI_D 3.141592653589793
+//
+// NNP::compute_symm (nnp/nnp.cpp:350-392) with every term and sum in FP64,
+// for potentials whose input scaling amplifies the FP32 rounding of the
+// terms (nnp_set_accumulation(NNP_SYMM_FP64)).  The displacement of each
+// neighbour is recovered in FP64 from the wrapped positions: the FP32 record
+// d32 = x_i - x_j - R q fixes the integer image q = round(B (x_i - x_j - d32)).
+// The basis functions are the FP64 formulas of Cutoff::cutf
+// (cutoff.cpp:62-114), BasisR::symmf (basis_radial.cpp:175-257) and
+// BasisA::symmf (basis_angular.cpp:212-260), the GAUSS damping width shared
+// by a run of equal eta as in BasisA::init (basis_angular.cpp:178-205).
+// One warp per atom; the rows are stored as FP32.
+
+__device__ __forceinline__ double cutf64(int name, double r, double rc)
+{
+    if (!(r < rc)) return 0.0;
+    switch (name) {
+    case CUT_STEP: return 1.0;
+    case CUT_COS: return 0.5 * (cospi(r / rc) + 1.0);
+    case CUT_TANH: { const double t = tanh(1.0 - r / rc); return t * t * t; }
+    case CUT_POLY3: { const double x = r / rc; return (2.0 * x - 3.0) * x * x + 1.0; }
+    default: return 0.0;
+    }
+}
+
+__device__ __forceinline__ double radial64(int form, double r, double rs, double eta, double fc)
+{
+    const double x = eta * (r - rs);
+    switch (form) {
+    case RAD_GAUSSIAN: return exp(-x * x) * fc;
+    case RAD_SECH: { const double e = exp(-fabs(x)); return 2.0 * e / (1.0 + e * e) * fc; }
+    case RAD_LOGISTIC: { const double e = exp(-fabs(x)), s = 2.0 * e / (1.0 + e * e); return s * s * fc; }
+    case RAD_TANH: return 0.5 * (tanh(-x) + 1.0) * fc;
+    case RAD_LOGCOSH: {
+        const double y = -2.0 * x;
+        return 0.5 * ((y > 0.0) ? y + log1p(exp(-y)) : log1p(exp(y))) * fc;
+    }
+    case RAD_LOGCOSH2: {
+        const double k = 2.0 * 1.4142135623730951, a = -x;
+        const double f = (fabs(a) < 1e-6) ? 1.0 / k + 0.5 * a + k * a * a / 12.0 : a / (-expm1(-k * a));
+        return f * fc;
+    }
+    default: return 0.0;
+    }
+}
+
+__device__ __forceinline__ double ipow64(double x, int n)
+{
+    double r = 1.0;
+    while (n) {
+        if (n & 1) r *= x;
+        x *= x;
+        n >>= 1;
+    }
+    return r;
+}
+
+// (lf, zeta, ieta2) of one angular function: value for a pair with cosine cs,
+// r_j^2 + r_k^2 = r2s and cutoff product cc
+__device__ __forceinline__ double angular64(int form, double cs, double r2s, double cc, double lf, double zeta,
+                                            double ieta2)
+{
+    const double cw = fabs(0.5 + lf * cs);
+    const double pz = (zeta == floor(zeta) && zeta >= 0.0 && zeta <= 64.0) ? ipow64(cw, (int)zeta) : pow(cw, zeta);
+    double rad;
+    switch (form) {
+    case ANG_GAUSS: rad = exp(-ieta2 * r2s); break;
+    case ANG_GAUSS2: { const double fd = exp(-0.5 * NNP_PI_D * ieta2 * r2s); rad = 2.0 * fd / (1.0 + fd); } break;
+    case ANG_SECH: { const double fd = exp(-0.5 * NNP_PI_D * ieta2 * r2s); rad = 2.0 * fd / (1.0 + fd * fd); } break;
+    case ANG_STUDENT3: case ANG_STUDENT4: case ANG_STUDENT5:
+        rad = ipow64(1.0 / sqrt(1.0 + ieta2 * r2s), 4 + (form - ANG_STUDENT3));
+        break;
+    default: rad = 0.0;
+    }
+    return pz * rad * cc;
+}
+
+__device__ __forceinline__ double warp_sum64(double v)
+{
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// shared memory per warp: r, ux, uy, uz and NNP_MAX_CUT cutoff values per
+// neighbour slot (doubles), then the neighbour's type (int)
+__host__ __device__ inline size_t symm64_floats(int cap) { return (size_t)cap * (2 * (4 + NNP_MAX_CUT) + 1) + 8; }
+
+__global__ void __launch_bounds__(WARPS * 32) k_symm_f64(int64_t N, const DevPot *__restrict__ pot,
+                                                          const double2 *__restrict__ rpar64,
+                                                          const double4 *__restrict__ apar64,
+                                                          const double *__restrict__ cut_rc,
+                                                          const int *__restrict__ type, const int *__restrict__ order,
+                                                          const float4 *__restrict__ nbr,
+                                                          const int *__restrict__ nbr_cnt, int cap,
+                                                          const double *__restrict__ xw,
+                                                          const int *__restrict__ atom_struct,
+                                                          const StructGrid *__restrict__ grid, int gstride,
+                                                          float *__restrict__ G)
+{
+    extern __shared__ double sm64[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *base = sm64 + (size_t)warp * (symm64_floats(cap) / 2 + 4);
+    double *R = base, *UX = R + cap, *UY = UX + cap, *UZ = UY + cap, *FC = UZ + cap;   // FC[c * cap + k]
+    int *TY = reinterpret_cast<int *>(FC + NNP_MAX_CUT * cap);
+    const DevPot &P = *pot;
+    for (int64_t idx = blockIdx.x * (int64_t)WARPS + warp; idx < N; idx += (int64_t)gridDim.x * WARPS) {
+        const int64_t i = order[idx];
+        const int II = type[i];
+        if ((unsigned)II >= (unsigned)P.ntypes) continue;
+        const DevType &T = P.t[II];
+        const int n = min(nbr_cnt[i], cap);
+        const StructGrid &g = grid[atom_struct[i]];
+        const double xi0 = xw[3 * i], xi1 = xw[3 * i + 1], xi2 = xw[3 * i + 2];
+        for (int k = lane; k < n; k += 32) {
+            const float4 rec = nbr[i * cap + k];
+            const int jt = __float_as_int(rec.w), j = jt & 0x0fffffff;
+            const double sx = xi0 - xw[3 * (int64_t)j], sy = xi1 - xw[3 * (int64_t)j + 1],
+                         sz = xi2 - xw[3 * (int64_t)j + 2];
+            double dx = sx, dy = sy, dz = sz;
+            if (g.pbc) {
+                const double ex = sx - rec.x, ey = sy - rec.y, ez = sz - rec.z;     // R q
+                double q[3];
+                for (int m = 0; m < 3; ++m) q[m] = rint(g.B[3 * m] * ex + g.B[3 * m + 1] * ey + g.B[3 * m + 2] * ez);
+                dx -= g.R[0] * q[0] + g.R[3] * q[1] + g.R[6] * q[2];
+                dy -= g.R[1] * q[0] + g.R[4] * q[1] + g.R[7] * q[2];
+                dz -= g.R[2] * q[0] + g.R[5] * q[1] + g.R[8] * q[2];
+            }
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            R[k] = r;
+            UX[k] = dx / r;
+            UY[k] = dy / r;
+            UZ[k] = dz / r;
+            for (int c = 0; c < P.ncut; ++c) FC[c * cap + k] = cutf64(P.cut[c].name, r, cut_rc[c]);
+            TY[k] = jt >> 28;
+        }
+        __syncwarp();
+        // neighbours are grouped by type: segment [s0, s1) of type J
+        int seg[NNP_MAX_TYPES + 1];
+        {
+            int c = 0;
+            for (int J = 0; J < P.ntypes; ++J) {
+                seg[J] = c;
+                int cnt = 0;
+                for (int k = lane; k < n; k += 32) cnt += (TY[k] == J);
+                c += __reduce_add_sync(FULL, cnt);
+            }
+            seg[P.ntypes] = c;
+        }
+        float *Gi = G + i * (int64_t)gstride;
+        for (int q = lane; q < gstride; q += 32) Gi[q] = 0.f;
+        __syncwarp();
+        // radial: lane f sums function f over the block's neighbours
+        for (int J = 0; J < P.ntypes; ++J) {
+            const DevBlockR B = T.br[J];
+            if (lane < B.n) {
+                const double2 q = rpar64[B.par + lane];
+                double acc = 0.0;
+                for (int k = seg[J]; k < seg[J + 1]; ++k)
+                    acc += radial64(B.form, R[k], q.x, q.y, FC[B.cut * cap + k]);
+                Gi[B.off_g + lane] = (float)acc;
+            }
+        }
+        // angular blocks tt = K (K + 1) / 2 + J, J <= K: lanes over the partner b of each first member a
+        for (int K = 0, tt = 0; K < P.ntypes; ++K)
+            for (int J = 0; J <= K; ++J, ++tt) {
+                const DevBlockA B = T.ba[tt];
+                if (B.n == 0) continue;
+                double acc[NNP_MAX_AFUNC];
+                for (int f = 0; f < B.n; ++f) acc[f] = 0.0;
+                for (int a = seg[J]; a < seg[J + 1]; ++a) {
+                    const int b0 = (J == K) ? a + 1 : seg[K];
+                    for (int b = b0 + lane; b < seg[K + 1]; b += 32) {
+                        const double cs = UX[a] * UX[b] + UY[a] * UY[b] + UZ[a] * UZ[b];
+                        const double r2s = R[a] * R[a] + R[b] * R[b];
+                        const double cc = FC[B.cut * cap + a] * FC[B.cut * cap + b];
+                        for (int f = 0; f < B.n; ++f) {
+                            const double4 q = apar64[B.par + f];
+                            acc[f] += angular64(B.form, cs, r2s, cc, q.x, q.y, q.z);
+                        }
+                    }
+                }
+                for (int f = 0; f < B.n; ++f) {
+                    const double v = warp_sum64(acc[f]);
+                    if (lane == 0) Gi[B.off_g + f] = (float)v;
+                }
+            }
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(WARPS * 32) k_nn_fp32(int64_t N, const DevPot *__restrict__ pot,
                                                        const float *__restrict__ wpar, int64_t wfloats,
                                                        const int *__restrict__ type, const float *__restrict__ G,
@@ -746,14 +984,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_force(int64_t N, const DevPot
 
 // ------------------------------------------------------------------ energies
 
-__global__ void k_energy(const int64_t *__restrict__ off, const float *__restrict__ e_atom,
+__global__ void k_energy(const int64_t *__restrict__ off, int64_t n_centre, const float *__restrict__ e_atom,
                          const int *__restrict__ type, const DevPot *__restrict__ pot, int vacuum,
                          const double *__restrict__ vac, double *__restrict__ e_struct, DevErr *err)
 {
     __shared__ double part[256];
     const int s = blockIdx.x;
     double sum = 0.0;
-    for (int64_t a = off[s] + threadIdx.x; a < off[s + 1]; a += blockDim.x) {
+    const int64_t a1 = off[s + 1] < n_centre ? off[s + 1] : n_centre;     // ghosts carry no energy
+    for (int64_t a = off[s] + threadIdx.x; a < a1; a += blockDim.x) {
         sum += (double)e_atom[a];
         if (vacuum) {
             const int t = type[a];
@@ -839,6 +1078,7 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
 {
     (void)pbc;
     E.n_atoms = n_atoms;
+    E.n_centre = n_atoms - std::min<int64_t>(std::max<int64_t>(E.n_ghost, 0), n_atoms);
     E.n_struct = n_struct;
     const size_t N = (size_t)std::max<int64_t>(n_atoms, 1), S = (size_t)std::max(n_struct, 1);
     const size_t cell_bound = 64 * S + 2 * N + 64;
@@ -848,6 +1088,7 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.atom_struct.reserve(N));
     r(E.atom_cell.reserve(N));
     r(E.grid.reserve(S));
+    r(E.bbox.reserve(6 * S));
     r(E.scan_tmp.reserve(S));
     r(E.cell_cnt.reserve(cell_bound));
     r(E.cell_start.reserve(cell_bound));
@@ -879,13 +1120,15 @@ std::string run_neighbors(Engine &E, int pbc)
     E.mark(0);
     E.launches += 12;
     cudaMemsetAsync(E.type_fill.p, 0, 2 * (NNP_MAX_TYPES + 1) * sizeof(int), st);
-    k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p);
-    k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.type.p, E.dpot.ntypes, E.type_fill.p,
+    k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p);
+    k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p,
                                                                E.type_fill.p + NNP_MAX_TYPES + 1, E.order.p);
     k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
                                                              E.dpot.ntypes, E.err.p);
+    if (!pbc) k_struct_bbox<<<S, 256, 0, st>>>(E.pos.p, E.atom_off.p, E.bbox.p);
     k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
-                                                              E.grid.p, E.scan_tmp.p, E.err.p);
+                                                              E.bbox.p, E.grid.p, E.scan_tmp.p, E.err.p);
+    E.launches += pbc ? 0 : 1;
     k_cell_base<<<1, 1024, 0, st>>>(E.scan_tmp.p, S, E.grid.p);
     const size_t cell_bound = 64 * (size_t)S + 2 * (size_t)N + 64;
     cudaMemsetAsync(E.cell_cnt.p, 0, cell_bound * sizeof(int), st);
@@ -909,12 +1152,12 @@ std::string run_neighbors(Engine &E, int pbc)
 
 std::string run_symm(Engine &E)
 {
-    const int64_t N = E.n_atoms;
+    const int64_t N = E.n_centre;      // centres: the first n_centre entries of `order`
     if (N == 0) return "";
     const size_t sm = view_bytes(E, false);
     const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
-    if (E.use_jit && E.jit_symm && !E.acc64) {
+    if (E.use_jit && E.jit_symm && !E.acc64 && !E.symm64) {
         long long n = N;
         int cap = E.cap, nc = ncut_max(E), nd = ndamp_max(E), gs = E.gstride;
         void *args[] = {&n, &E.d_pot, &E.rpar.p, &E.apar.p, &E.type.p, &E.order.p, &E.nbr.p, &E.nbr_cnt.p,
@@ -922,6 +1165,15 @@ std::string run_symm(Engine &E)
         std::string msg = jit_launch(E.jit_symm, grid, WARPS * 32, sm, E.stream, args);
         E.mark(2);
         return msg;
+    }
+    if (E.symm64) {
+        const size_t sm64 = (size_t)WARPS * (symm64_floats(E.cap) / 2 + 4) * sizeof(double);
+        cudaFuncSetAttribute(k_symm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64);
+        k_symm_f64<<<grid, WARPS * 32, sm64, E.stream>>>(N, E.d_pot, E.rpar64.p, E.apar64.p, E.cut64.p, E.type.p,
+                                                         E.order.p, E.nbr.p, E.nbr_cnt.p, E.cap, E.xw.p,
+                                                         E.atom_struct.p, E.grid.p, E.gstride, E.G.p);
+        E.mark(2);
+        return cuda_msg("symmetry functions (FP64)");
     }
     auto kern = E.acc64 ? k_symm<double> : k_symm<float>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -951,7 +1203,7 @@ std::string run_nn(Engine &E)
     if (sm > 220 * 1024) return "networks too large for the shared-memory FP32 path";
     cudaFuncSetAttribute(k_nn_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_nn_fp32<<<grid_for(N, WARPS * 8, num_sms() * 2), WARPS * 32, sm, E.stream>>>(
-        N, E.d_pot, E.wpar.p, E.wfloats, E.type.p, E.G.p, E.gstride, maxn, E.e_atom.p, E.dEdG.p);
+        E.n_centre, E.d_pot, E.wpar.p, E.wfloats, E.type.p, E.G.p, E.gstride, maxn, E.e_atom.p, E.dEdG.p);
     E.launches += 1;
     E.mark(3);
     return cuda_msg("networks");
@@ -959,9 +1211,9 @@ std::string run_nn(Engine &E)
 
 std::string run_force(Engine &E)
 {
-    const int64_t N = E.n_atoms;
-    if (N == 0) return "";
-    cudaMemsetAsync(E.force.p, 0, 3 * (size_t)N * sizeof(double), E.stream);
+    const int64_t N = E.n_centre;      // centres; forces are scattered onto every atom, ghosts included
+    if (E.n_atoms == 0) return "";
+    cudaMemsetAsync(E.force.p, 0, 3 * (size_t)E.n_atoms * sizeof(double), E.stream);
     double *vir = E.want_virial ? E.vir.p : nullptr;
     if (vir) cudaMemsetAsync(vir, 0, 9 * (size_t)E.n_struct * sizeof(double), E.stream);
     const size_t sm = view_bytes(E, true);
@@ -987,7 +1239,7 @@ std::string run_force(Engine &E)
 std::string run_energy(Engine &E, bool vacuum)
 {
     if (E.n_struct == 0) return "";
-    k_energy<<<E.n_struct, 256, 0, E.stream>>>(E.atom_off.p, E.e_atom.p, E.type.p, E.d_pot, vacuum ? 1 : 0,
+    k_energy<<<E.n_struct, 256, 0, E.stream>>>(E.atom_off.p, E.n_centre, E.e_atom.p, E.type.p, E.d_pot, vacuum ? 1 : 0,
                                                E.vac.p, E.e_struct.p, E.err.p);
     E.launches += 1;
     E.mark(5);
@@ -1007,7 +1259,7 @@ __global__ void k_atom_energy(int64_t N, const float *__restrict__ e_atom, const
 
 std::string run_atom_energy(Engine &E, bool vacuum, double *out)
 {
-    const int64_t N = E.n_atoms;
+    const int64_t N = E.n_centre;
     if (N == 0) return "";
     k_atom_energy<<<grid_for(N, 256, 1 << 30), 256, 0, E.stream>>>(N, E.e_atom.p, E.type.p, E.dpot.ntypes,
                                                                    vacuum ? 1 : 0, E.vac.p, out);

@@ -22,6 +22,7 @@ NNP_OK = 0
 ERRORS = {-1: "ARG", -2: "IO", -3: "PARSE", -4: "CUDA", -5: "CAPACITY", -6: "UNSUPPORTED", -7: "TYPE",
           -8: "NOT_FINITE"}
 PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
+ACC_FP32, ACC_FP64, SYMM_FP64 = 0, 1, 2
 LOSS_MSE, LOSS_MAE, LOSS_HUBER, LOSS_ASINH = 1, 2, 3, 4   # opt::Loss (opt/loss.hpp:18-24)
 ENERGY, FORCES, VACUUM, DEVICE_PTRS, SYMM = 1, 2, 4, 8, 16
 
@@ -61,6 +62,7 @@ def lib():
             "nnp_n_input": ([p, i, C.POINTER(i)], i),
             "nnp_compute": ([p, C.POINTER(_Batch), p, p, p, u], i),
             "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
+            "nnp_compute_local_ghost": ([p, C.c_int64, C.c_int64, p, p, p, p, p, p, u], i),
             "nnp_set_graphs": ([p, i], i),
             "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
             "nnp_nparams": ([p, i, C.POINTER(i)], i),
@@ -187,6 +189,22 @@ class NNP:
         """Bound of each tensor-core MMA-chain wait (0: the default)."""
         self._check(lib().nnp_set_mma_wait(self._h, int(polls)))
 
+    def compute_local_ghost(self, pos_local, type_local, pos_ghost, type_ghost, vacuum=False):
+        """One domain of a pair style: local atoms then ghost atoms, no cell.
+        Returns (energy of the local atoms, forces [n_local + n_ghost, 3],
+        per-atom energies [n_local], virial [3, 3])."""
+        pos = np.ascontiguousarray(np.concatenate([np.reshape(pos_local, (-1, 3)), np.reshape(pos_ghost, (-1, 3))]),
+                                   dtype=np.float64)
+        typ = np.ascontiguousarray(np.concatenate([np.asarray(type_local), np.asarray(type_ghost)]), dtype=np.int32)
+        nl, ng = len(pos_local), len(pos_ghost)
+        e = np.zeros(1)
+        f = np.zeros((max(nl + ng, 1), 3))
+        ea = np.zeros(max(nl, 1))
+        w = np.zeros(9)
+        self._check(lib().nnp_compute_local_ghost(self._h, nl, ng, _ptr(pos), _ptr(typ), _ptr(e), _ptr(f), _ptr(ea),
+                                                  _ptr(w), VACUUM if vacuum else 0))
+        return float(e[0]), f[:nl + ng], ea[:nl], w.reshape(3, 3)
+
     def set_autotune(self, on: bool = True):
         """Tune the kernels' launch and tile choices on the first energy+force
         call of each neighbour-capacity class (cached on disk)."""
@@ -207,9 +225,11 @@ class NNP:
         """Replay the device-side step as a CUDA graph while calls repeat their shape."""
         self._check(lib().nnp_set_graphs(self._h, 1 if on else 0))
 
-    def set_accumulation(self, fp64: bool = True):
-        """FP64 (default) or FP32 running sums of the symmetry functions."""
-        self._check(lib().nnp_set_accumulation(self._h, 1 if fp64 else 0))
+    def set_accumulation(self, mode=1):
+        """Precision of the symmetry functions: ACC_FP32 (0, or False), ACC_FP64
+        (1, or True: FP64 running sums of FP32 terms) or SYMM_FP64 (2: FP64
+        terms and sums)."""
+        self._check(lib().nnp_set_accumulation(self._h, int(mode)))
 
     def set_specialization(self, on: bool = True):
         """Use the kernels compiled for this basis at creation (True) or the prebuilt ones."""

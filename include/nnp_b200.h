@@ -100,11 +100,18 @@ int nnp_set_precision(nnp_handle *h, int32_t precision);
  * tensor memory, so the handle stays usable. */
 int nnp_set_mma_wait(nnp_handle *h, int64_t polls);
 
-/* Running sums of the symmetry functions: NNP_ACC_FP64 adds every
- * FP32 pair/triplet term into an FP64 sum; NNP_ACC_FP32 (default) keeps FP32 sums
- * (faster; ~sqrt(T/32) ulp error for T triplets per atom). */
+/* Precision of the symmetry functions: NNP_ACC_FP32 (default) computes every
+ * pair/triplet term and running sum in FP32; NNP_ACC_FP64 adds the FP32 terms
+ * into FP64 sums (~sqrt(T/32) ulp less error for T triplets per atom);
+ * NNP_SYMM_FP64 evaluates the terms themselves in FP64 (neighbour
+ * displacements recovered in FP64 from the positions, FP64 basis functions
+ * and parameters, prebuilt kernel), storing the rows as FP32.  Networks and
+ * forces stay FP32 in every mode.  NNP_SYMM_FP64 is for potentials whose
+ * input scaling (inpw) is large enough to turn the ~1e-7 relative FP32 error
+ * of the terms into force errors above 1e-5 eV/A; it is several times slower. */
 #define NNP_ACC_FP32 0
 #define NNP_ACC_FP64 1
+#define NNP_SYMM_FP64 2
 int nnp_set_accumulation(nnp_handle *h, int32_t acc);
 
 /* Kernels specialised for the loaded basis.  At creation the library writes
@@ -193,6 +200,26 @@ int nnp_compute(nnp_handle *h, const nnp_batch *batch, double *energy, double *f
  * flags: NNP_VACUUM, NNP_DEVICE_PTRS. */
 int nnp_compute_md(nnp_handle *h, const nnp_batch *batch, double *energy, double *forces, double *atom_energy,
                    double *virial, uint32_t flags);
+
+/* Force call of a LAMMPS-style pair style on one spatial domain (the
+ * reference's ML-ATOMNN pair style, README.md:376-380, is not in its
+ * sources): n_local owned atoms followed by n_ghost ghost atoms (periodic
+ * images and neighbouring domains' atoms within rc of the domain, as the
+ * caller's communication provides them), no cell.  Only local atoms are
+ * centres: the energy is the sum of their atomic energies; ghosts enter
+ * only as neighbours.  Forces are written for every atom, ghosts included
+ * (-dE/dx_ghost, to be added to the owning atom by the caller's reverse
+ * communication, as a pair style with newton on does).
+ *  pos[3*(n_local+n_ghost)], type[n_local+n_ghost]   host arrays
+ *  energy[1]                  sum of the local atoms' energies (+ vacuum with NNP_VACUUM)
+ *  forces[3*(n_local+n_ghost)]
+ *  atom_energy[n_local]       per-atom energies of the local atoms
+ *  virial[9]                  W = -dE/d(strain) of the domain's pair terms
+ *                             (sum over all atoms of x_i (x) F_i), as nnp_compute_md
+ * Any output may be NULL.  flags: NNP_VACUUM. */
+int nnp_compute_local_ghost(nnp_handle *h, int64_t n_local, int64_t n_ghost, const double *pos,
+                            const int32_t *type, double *energy, double *forces, double *atom_energy,
+                            double *virial, uint32_t flags);
 
 /* Energy of every structure from precomputed symmetry functions; replaces
  * NNP::compute_energy (nnp.cpp:329-338) with NNH::energy (nnh.cpp:207-210):
