@@ -894,6 +894,77 @@ int nnp_compute_md(nnp_handle *h, const nnp_batch *b, double *energy, double *fo
     return compute_impl(h, b, energy, forces, nullptr, atom_energy, virial, flags);
 }
 
+int nnp_input_stats(nnp_handle *h, const nnp_batch *batch, int64_t *count, double *stats)
+{
+    if (!h || !batch || !count || !stats) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (batch->n_struct <= 0) return fail(h, NNP_ERR_ARG, "empty batch");
+    // neighbour lists and symmetry functions of the batch (no networks)
+    int rc = compute_impl(h, batch, nullptr, nullptr, nullptr, nullptr, nullptr, 0u);
+    if (rc != NNP_OK) return rc;
+    std::vector<int64_t> c;
+    std::vector<double> st;
+    const std::string msg = nnp::run_input_stats(E, c, st);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    std::copy(c.begin(), c.end(), count);
+    std::copy(st.begin(), st.end(), stats);
+    return NNP_OK;
+}
+
+int nnp_precondition(nnp_handle *h, const nnp_batch *batch, int32_t prebias, int32_t prescale, double inbias,
+                     double inscale)
+{
+    if (!h || !batch) return NNP_ERR_ARG;
+    if (prebias < NNP_PREBIAS_IDENTITY || prebias > NNP_PREBIAS_MIN) return fail(h, NNP_ERR_ARG, "Invalid input bias.");
+    if (prescale < NNP_PRESCALE_IDENTITY || prescale > NNP_PRESCALE_MAX)
+        return fail(h, NNP_ERR_ARG, "Invalid input scaling.");
+    nnp::Engine &E = h->E;
+    const int T = E.host.ntypes(), gs = E.gstride;
+    std::vector<int64_t> cnt(T);
+    std::vector<double> st((size_t)T * NNP_NSTATS * gs);
+    int rc = nnp_input_stats(h, batch, cnt.data(), st.data());
+    if (rc != NNP_OK) return rc;
+    auto S = [&](int t, int s, int k) { return st[((size_t)t * NNP_NSTATS + s) * gs + k]; };
+    for (int t = 0; t < T; ++t) {
+        nnp::HostNet &net = E.host.nets[t];
+        const int nin = (int)net.inpb.size();
+        for (int k = 0; k < nin; ++k) {
+            double b = 0.0;
+            switch (prebias) {
+            case NNP_PREBIAS_MEAN: b = -S(t, NNP_STAT_MEAN, k); break;
+            case NNP_PREBIAS_HAR: b = -S(t, NNP_STAT_HARMONIC, k); break;
+            case NNP_PREBIAS_RMS: b = -S(t, NNP_STAT_RMS, k); break;
+            case NNP_PREBIAS_MID: b = -0.5 * (S(t, NNP_STAT_MAX, k) + S(t, NNP_STAT_MIN, k)); break;
+            case NNP_PREBIAS_MIN: b = -S(t, NNP_STAT_MIN, k); break;
+            default: b = 0.0; break;
+            }
+            double w = 1.0;
+            switch (prescale) {
+            case NNP_PRESCALE_DEV: {
+                const double d = S(t, NNP_STAT_DEV, k);
+                w = (d == 0) ? 1.0 : 1.0 / d;
+            } break;
+            case NNP_PRESCALE_MINMAX: {
+                const double d = S(t, NNP_STAT_MAX, k) - S(t, NNP_STAT_MIN, k);
+                w = (d > 0) ? 1.0 / d : 1.0;
+            } break;
+            case NNP_PRESCALE_MAX: {
+                const double d = S(t, NNP_STAT_MAX, k);
+                w = (d > 0) ? 1.0 / d : 1.0;
+            } break;
+            default: w = 1.0; break;
+            }
+            net.inpb[k] = b + inbias;
+            net.inpw[k] = w * inscale;
+        }
+        for (auto &v : net.outb) v = 0.0;
+        for (auto &v : net.outw) v = 1.0;
+    }
+    const std::string msg = E.upload();
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    return NNP_OK;
+}
+
 int nnp_compute_local_ghost(nnp_handle *h, int64_t n_local, int64_t n_ghost, const double *pos,
                             const int32_t *type, double *energy, double *forces, double *atom_energy, double *virial,
                             uint32_t flags)

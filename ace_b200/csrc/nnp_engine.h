@@ -178,6 +178,7 @@ std::string run_atom_energy(Engine &E, bool vacuum, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
 std::string run_train_grad(Engine &E, bool with_force);
+std::string run_input_stats(Engine &E, std::vector<int64_t> &count, std::vector<double> &stats);
 int tc_smem_bytes(const Engine &E, bool split);     // 0: networks do not fit the tensor-core path
 std::string run_nn_tc(Engine &E, bool split);
 std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,

@@ -24,6 +24,9 @@ ERRORS = {-1: "ARG", -2: "IO", -3: "PARSE", -4: "CUDA", -5: "CAPACITY", -6: "UNS
 PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
 ACC_FP32, ACC_FP64, SYMM_FP64 = 0, 1, 2
 LOSS_MSE, LOSS_MAE, LOSS_HUBER, LOSS_ASINH = 1, 2, 3, 4   # opt::Loss (opt/loss.hpp:18-24)
+STATS = ("max", "min", "harmonic", "mean", "dev", "rms")   # nnp_input_stats, NNP_STAT_* order
+PREBIAS = {"IDENTITY": 0, "MEAN": 1, "HAR": 2, "RMS": 3, "MID": 4, "MIN": 5}      # nnptefr.hpp:97-107
+PRESCALE = {"IDENTITY": 0, "DEV": 1, "MINMAX": 2, "MAX": 3}                     # nnptefr.hpp:69-77
 ENERGY, FORCES, VACUUM, DEVICE_PTRS, SYMM = 1, 2, 4, 8, 16
 
 
@@ -63,6 +66,8 @@ def lib():
             "nnp_compute": ([p, C.POINTER(_Batch), p, p, p, u], i),
             "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
             "nnp_compute_local_ghost": ([p, C.c_int64, C.c_int64, p, p, p, p, p, p, u], i),
+            "nnp_input_stats": ([p, C.POINTER(_Batch), p, p], i),
+            "nnp_precondition": ([p, C.POINTER(_Batch), i, i, d, d], i),
             "nnp_set_graphs": ([p, i], i),
             "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
             "nnp_nparams": ([p, i, C.POINTER(i)], i),
@@ -188,6 +193,38 @@ class NNP:
     def set_mma_wait(self, polls: int):
         """Bound of each tensor-core MMA-chain wait (0: the default)."""
         self._check(lib().nnp_set_mma_wait(self._h, int(polls)))
+
+    def _batch(self, atom_off, pos, types, cells, pbc):
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        S = len(atom_off) - 1
+        cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(S, 9) if pbc else None
+        keep = (atom_off, pos, types, cells)
+        return _Batch(S, atom_off.ctypes.data, pos.ctypes.data, types.ctypes.data,
+                      cells.ctypes.data if cells is not None else None, 1 if pbc else 0), keep
+
+    def input_stats(self, atom_off, pos, types, cells, pbc=True):
+        """Per-element statistics of the network inputs over a batch
+        (nnptefr.cpp:689-781): (count [ntypes], {name: array [ntypes, gstride]})."""
+        b, keep = self._batch(atom_off, pos, types, cells, pbc)
+        T = self.ntypes
+        gs = max(self.n_input(t) for t in range(T))
+        gs = (gs + 3) & ~3
+        cnt = np.zeros(T, dtype=np.int64)
+        st = np.zeros((T, len(STATS), gs))
+        self._check(lib().nnp_input_stats(self._h, C.byref(b), _ptr(cnt), _ptr(st)))
+        return cnt, {name: st[:, k, :] for k, name in enumerate(STATS)}
+
+    def precondition(self, atom_off, pos, types, cells, prebias="MEAN", prescale="DEV", inbias=0.0, inscale=1.0,
+                     pbc=True):
+        """nnptefr's input preconditioning (nnptefr.cpp:783-880) from the batch's statistics."""
+        b, keep = self._batch(atom_off, pos, types, cells, pbc)
+        pb = PREBIAS.get(prebias, prebias) if isinstance(prebias, str) else prebias
+        ps = PRESCALE.get(prescale, prescale) if isinstance(prescale, str) else prescale
+        self._check(lib().nnp_precondition(self._h, C.byref(b), int(pb) if not isinstance(pb, str) else 99,
+                                           int(ps) if not isinstance(ps, str) else 99, float(inbias),
+                                           float(inscale)))
 
     def compute_local_ghost(self, pos_local, type_local, pos_ghost, type_ghost, vacuum=False):
         """One domain of a pair style: local atoms then ghost atoms, no cell.

@@ -253,6 +253,48 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);
 
+/* Input statistics of the networks over a training set: NNPTEFR::train's
+ * statistics of the symmetry functions per element (nnptefr.cpp:689-781),
+ * computed on the device from the batch's symmetry functions (the
+ * accumulation mode of nnp_set_accumulation applies).
+ *  count[ntypes]                         atoms of each element
+ *  stats[(t*NNP_NSTATS + s)*gstride + k] statistic s of input k of element t,
+ *                                        gstride = max nnp_n_input (the rest is 0):
+ *   NNP_STAT_MAX, NNP_STAT_MIN, NNP_STAT_HARMONIC (N / sum 1/G), NNP_STAT_MEAN,
+ *   NNP_STAT_DEV (sqrt(sum (mean - G)^2 / (N - 1))), NNP_STAT_RMS (sqrt(sum G^2 / N)).
+ * Host pointers. */
+#define NNP_NSTATS 6
+#define NNP_STAT_MAX 0
+#define NNP_STAT_MIN 1
+#define NNP_STAT_HARMONIC 2
+#define NNP_STAT_MEAN 3
+#define NNP_STAT_DEV 4
+#define NNP_STAT_RMS 5
+int nnp_input_stats(nnp_handle *h, const nnp_batch *batch, int64_t *count, double *stats);
+
+/* Preconditioning of the network inputs from those statistics, as nnptefr
+ * does before training (nnptefr.cpp:783-880): per element
+ *   inpb = -(statistic of prebias) + inbias, inpw = (1 / statistic of prescale) * inscale,
+ * outb = 0, outw = 1.  prebias: PreBias (nnptefr.hpp:97-107) IDENTITY 0 (inpb = 0),
+ * MEAN 1, HAR 2, RMS 3, MID 4 ((max+min)/2), MIN 5; prescale: PreScale
+ * (nnptefr.hpp:69-77) IDENTITY 0 (inpw = 1), DEV 1, MINMAX 2 (max - min), MAX 3;
+ * a zero (DEV, MINMAX) or non-positive (MAX) statistic gives scale 1.
+ * The reference's NONE values (6, 4) are rejected like the reference rejects
+ * them ("Invalid input bias." / "Invalid input scaling.").  The handle's
+ * networks are updated in place; nnp_write writes them. */
+#define NNP_PREBIAS_IDENTITY 0
+#define NNP_PREBIAS_MEAN 1
+#define NNP_PREBIAS_HAR 2
+#define NNP_PREBIAS_RMS 3
+#define NNP_PREBIAS_MID 4
+#define NNP_PREBIAS_MIN 5
+#define NNP_PRESCALE_IDENTITY 0
+#define NNP_PRESCALE_DEV 1
+#define NNP_PRESCALE_MINMAX 2
+#define NNP_PRESCALE_MAX 3
+int nnp_precondition(nnp_handle *h, const nnp_batch *batch, int32_t prebias, int32_t prescale, double inbias,
+                     double inscale);
+
 /* Energy-loss kind of nnp_train_grad, opt::Loss (opt/loss.hpp:18-24) as
  * NNPTEFR::error_cost_o1 applies it to dU = norm_s (E_s - e_ref_s)
  * (nnptefr.cpp:1340-1376): MSE 0.5 dU^2 (the default), MAE |dU|,
