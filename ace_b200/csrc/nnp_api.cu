@@ -965,6 +965,49 @@ int nnp_precondition(nnp_handle *h, const nnp_batch *batch, int32_t prebias, int
     return NNP_OK;
 }
 
+int nnp_taylor_expand(int32_t n_struct, const int64_t *atom_off, const double *pos, const int32_t *type,
+                      const double *energy, const double *forces, int32_t nadd, int32_t dist, double rdelta,
+                      uint64_t seed, int64_t *out_atom_off, double *out_pos, int32_t *out_type, double *out_energy,
+                      int32_t *out_src, int32_t *n_out)
+{
+    auto bad = [](int code, const std::string &m) {
+        g_create_error = m;
+        return code;
+    };
+    if (n_struct < 0 || nadd < 0 || !n_out) return bad(NNP_ERR_ARG, "bad structure count, copy count or output");
+    if (n_struct > 0 && (!atom_off || !pos || !type || !energy || !forces))
+        return bad(NNP_ERR_ARG, "input array missing");
+    if (!out_atom_off || !out_pos || !out_type || !out_energy || !out_src) return bad(NNP_ERR_ARG, "output array missing");
+    if (!(dist == 1 || dist == 2 || dist == 3 || dist == 5 || dist == 6 || dist == 7))
+        return bad(NNP_ERR_ARG, "Invalid position distribution.");
+    if (!(rdelta >= 0.0) || !std::isfinite(rdelta)) return bad(NNP_ERR_ARG, "rdelta must be finite and non-negative");
+    if (n_struct == 0) {
+        out_atom_off[0] = 0;
+        *n_out = 0;
+        return NNP_OK;
+    }
+    if (atom_off[0] != 0) return bad(NNP_ERR_ARG, "atom_off[0] must be 0");
+    for (int s = 0; s < n_struct; ++s)
+        if (atom_off[s + 1] < atom_off[s]) return bad(NNP_ERR_ARG, "atom_off must be non-decreasing");
+    std::vector<int64_t> oo;
+    std::vector<int> src;
+    std::vector<double> op, oe;
+    const std::string msg = nnp::taylor_expand(n_struct, atom_off, pos, energy, forces, nadd, dist, rdelta, seed, oo,
+                                               src, op, oe);
+    if (!msg.empty()) return bad(NNP_ERR_CUDA, msg);
+    const int O = (int)src.size();
+    std::copy(oo.begin(), oo.end(), out_atom_off);
+    std::copy(op.begin(), op.end(), out_pos);
+    std::copy(oe.begin(), oe.end(), out_energy);
+    for (int o = 0; o < O; ++o) {
+        out_src[o] = src[o];
+        const int64_t a0 = atom_off[src[o]], n = atom_off[src[o] + 1] - a0;
+        std::copy(type + a0, type + a0 + n, out_type + oo[o]);
+    }
+    *n_out = O;
+    return NNP_OK;
+}
+
 int nnp_compute_local_ghost(nnp_handle *h, int64_t n_local, int64_t n_ghost, const double *pos,
                             const int32_t *type, double *energy, double *forces, double *atom_energy, double *virial,
                             uint32_t flags)

@@ -179,6 +179,10 @@ std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
 std::string run_train_grad(Engine &E, bool with_force);
 std::string run_input_stats(Engine &E, std::vector<int64_t> &count, std::vector<double> &stats);
+std::string taylor_expand(int S, const int64_t *atom_off, const double *pos, const double *energy,
+                          const double *forces, int nadd, int dist, double rdelta, uint64_t seed,
+                          std::vector<int64_t> &out_off, std::vector<int> &out_src, std::vector<double> &out_pos,
+                          std::vector<double> &out_energy);
 int tc_smem_bytes(const Engine &E, bool split);     // 0: networks do not fit the tensor-core path
 std::string run_nn_tc(Engine &E, bool split);
 std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *off, const int *type,

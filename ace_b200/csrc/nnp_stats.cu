@@ -181,3 +181,169 @@ std::string run_input_stats(Engine &E, std::vector<int64_t> &count, std::vector<
 }
 
 }  // namespace nnp
+
+// ------------------------------------------------------------------ Taylor expansion of the training set
+//
+// NNPTEFR's force perturbation (nnptefr.cpp:2733-2830): every structure whose
+// mean force norm exceeds 1e-12 gets nadd copies in which each atom moves by
+// dr = vr (sin t cos p, sin t sin p, cos t), cos t and p / pi uniform in
+// (-1, 1), vr drawn from a distribution of width rdelta, and the copy's
+// energy is the first-order estimate E - sum_j dr_j . F_j.  The random numbers
+// come from a counter-based hash of (seed, output structure, atom, draw), so
+// a copy does not depend on the order in which the GPU makes it.
+
+namespace nnp {
+
+namespace {
+
+__host__ __device__ inline uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// uniform double in (0, 1) of draw k of atom j of output structure o
+__host__ __device__ inline double taylor_uniform(uint64_t seed, int64_t o, int64_t j, int k)
+{
+    const uint64_t h = mix64(mix64(mix64(seed + 0x9e3779b97f4a7c15ull) ^ (uint64_t)o) ^ ((uint64_t)j * 4 + (uint64_t)k));
+    return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// radius of the displacement: the inverse-CDF draws of rng::dist (math/random.cpp:64-146)
+// with location 0 and width w
+__device__ inline double taylor_radius(int dist, double w, double u1, double u2)
+{
+    const double pi = 3.141592653589793;
+    switch (dist) {
+    case 1: return u1 * w;                                                    // UNIFORM(0, w)
+    case 2: { const double p = u1 - 0.5; return -w * ((p > 0) - (p < 0)) * log(1.0 - 2.0 * fabs(p)); }   // LAPLACE
+    case 3: return w * sqrt(-2.0 * log(u1)) * cos(2.0 * pi * u2);            // NORMAL (Box-Muller)
+    case 5: return w * 2.0 / pi * log(tan(0.5 * pi * u1));                    // SECH
+    case 6: return w * log(u1 / (1.0 - u1));                                  // LOGISTIC
+    case 7: {                                                                 // COSINE (the reference's fit of its inverse CDF)
+        if (u1 < 0.5) {
+            const double t = sqrt(-2.0 * log(u1));
+            return w * (0.820251 - 0.806770 * t + 0.093247 * t * t);
+        }
+        const double t = sqrt(-2.0 * log(1.0 - u1));
+        return -w * (0.820251 - 0.806770 * t + 0.093247 * t * t);
+    }
+    default: return 0.0;
+    }
+}
+
+// one block per output structure: copy m of source structure src[o]
+__global__ void k_taylor(const int64_t *__restrict__ off, const double *__restrict__ pos,
+                         const double *__restrict__ energy, const double *__restrict__ forces,
+                         const int *__restrict__ src, const int *__restrict__ copy, const int64_t *__restrict__ out_off,
+                         int dist, double rdelta, uint64_t seed, double *__restrict__ out_pos,
+                         double *__restrict__ out_energy)
+{
+    __shared__ double red[256];
+    const int64_t o = blockIdx.x;
+    const int s = src[o];
+    const bool perturb = copy[o] > 0;
+    const int64_t a0 = off[s], n = off[s + 1] - a0, b0 = out_off[o];
+    double de = 0.0;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const double *x = pos + 3 * (a0 + j);
+        double *y = out_pos + 3 * (b0 + j);
+        if (!perturb) {
+            y[0] = x[0];
+            y[1] = x[1];
+            y[2] = x[2];
+            continue;
+        }
+        const double vr = taylor_radius(dist, rdelta, taylor_uniform(seed, o, j, 0), taylor_uniform(seed, o, j, 3));
+        const double ct = 2.0 * taylor_uniform(seed, o, j, 1) - 1.0, st = sqrt(1.0 - ct * ct);
+        const double ph = (2.0 * taylor_uniform(seed, o, j, 2) - 1.0) * 3.141592653589793;
+        const double d[3] = {vr * st * cos(ph), vr * st * sin(ph), vr * ct};
+        const double *f = forces + 3 * (a0 + j);
+        for (int k = 0; k < 3; ++k) y[k] = x[k] + d[k];
+        de += d[0] * f[0] + d[1] * f[1] + d[2] * f[2];
+    }
+    red[threadIdx.x] = de;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out_energy[o] = energy[s] - red[0];
+}
+
+}  // namespace
+
+// Host part: the output layout (originals in order, each followed by its
+// copies), the copy of the inputs to the device, the kernel and the copy
+// back.  Returns "" or an error message.
+std::string taylor_expand(int S, const int64_t *atom_off, const double *pos, const double *energy,
+                          const double *forces, int nadd, int dist, double rdelta, uint64_t seed,
+                          std::vector<int64_t> &out_off, std::vector<int> &out_src, std::vector<double> &out_pos,
+                          std::vector<double> &out_energy)
+{
+    const int64_t N = atom_off[S];
+    std::vector<int> src, cp;
+    out_off.assign(1, 0);
+    for (int s = 0; s < S; ++s) {
+        const int64_t a0 = atom_off[s], n = atom_off[s + 1] - a0;
+        double favg = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            const double *f = forces + 3 * (a0 + j);
+            favg += std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+        }
+        favg = n > 0 ? favg / (double)n : 0.0;
+        const int copies = favg > 1.0e-12 ? nadd : 0;
+        for (int m = 0; m <= copies; ++m) {
+            src.push_back(s);
+            cp.push_back(m);
+            out_off.push_back(out_off.back() + n);
+        }
+    }
+    const int O = (int)src.size();
+    const int64_t NO = out_off.back();
+    out_src = src;
+    out_pos.assign(3 * (size_t)NO, 0.0);
+    out_energy.assign(O, 0.0);
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return "cudaStreamCreate failed";
+    DBuf<int64_t> d_off, d_oo;
+    DBuf<double> d_pos, d_e, d_f, d_opos, d_oe;
+    DBuf<int> d_src, d_cp;
+    cudaError_t e = cudaSuccess;
+    auto r = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
+    r(d_off.reserve(S + 1));
+    r(d_oo.reserve(O + 1));
+    r(d_pos.reserve(3 * (size_t)std::max<int64_t>(N, 1)));
+    r(d_f.reserve(3 * (size_t)std::max<int64_t>(N, 1)));
+    r(d_e.reserve(S));
+    r(d_opos.reserve(3 * (size_t)std::max<int64_t>(NO, 1)));
+    r(d_oe.reserve(O));
+    r(d_src.reserve(O));
+    r(d_cp.reserve(O));
+    if (e == cudaSuccess) {
+        r(cudaMemcpyAsync(d_off.p, atom_off, sizeof(int64_t) * (S + 1), cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_oo.p, out_off.data(), sizeof(int64_t) * (O + 1), cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_f.p, forces, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_e.p, energy, sizeof(double) * S, cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_src.p, src.data(), sizeof(int) * O, cudaMemcpyHostToDevice, st));
+        r(cudaMemcpyAsync(d_cp.p, cp.data(), sizeof(int) * O, cudaMemcpyHostToDevice, st));
+    }
+    if (e == cudaSuccess && O > 0) {
+        k_taylor<<<O, 256, 0, st>>>(d_off.p, d_pos.p, d_e.p, d_f.p, d_src.p, d_cp.p, d_oo.p, dist, rdelta, seed,
+                                    d_opos.p, d_oe.p);
+        r(cudaGetLastError());
+    }
+    if (e == cudaSuccess) {
+        r(cudaMemcpyAsync(out_pos.data(), d_opos.p, sizeof(double) * 3 * NO, cudaMemcpyDeviceToHost, st));
+        r(cudaMemcpyAsync(out_energy.data(), d_oe.p, sizeof(double) * O, cudaMemcpyDeviceToHost, st));
+        r(cudaStreamSynchronize(st));
+    }
+    d_off.release(); d_oo.release(); d_pos.release(); d_f.release(); d_e.release();
+    d_opos.release(); d_oe.release(); d_src.release(); d_cp.release();
+    cudaStreamDestroy(st);
+    return e == cudaSuccess ? "" : std::string("Taylor expansion: ") + cudaGetErrorString(e);
+}
+
+}  // namespace nnp

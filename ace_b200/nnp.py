@@ -67,6 +67,7 @@ def lib():
             "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
             "nnp_compute_local_ghost": ([p, C.c_int64, C.c_int64, p, p, p, p, p, p, u], i),
             "nnp_input_stats": ([p, C.POINTER(_Batch), p, p], i),
+            "nnp_taylor_expand": ([i, p, p, p, p, p, i, i, d, C.c_uint64, p, p, p, p, p, C.POINTER(i)], i),
             "nnp_precondition": ([p, C.POINTER(_Batch), i, i, d, d], i),
             "nnp_set_graphs": ([p, i], i),
             "nnp_compute_energy_symm": ([p, i, p, p, p, i, p], i),
@@ -439,3 +440,34 @@ def tune_cache_load(key: str):
     v = np.zeros(5, dtype=np.int32)
     rc = lib().nnp_tune_cache_load(key.encode(), _ptr(v), 5)
     return None if rc != NNP_OK else dict(zip(NNP.TUNE_NAMES, (int(x) for x in v)))
+
+
+DISTRIBUTIONS = {"UNIFORM": 1, "LAPLACE": 2, "NORMAL": 3, "SECH": 5, "LOGISTIC": 6, "COSINE": 7}   # rng::dist::Name
+
+
+def taylor_expand(atom_off, pos, types, energy, forces, nadd, dist="NORMAL", rdelta=0.01, seed=0):
+    """nnptefr's force perturbation on the GPU (nnptefr.cpp:2733-2830):
+    returns (atom_off, pos [N',3], types [N'], energy [S'], source structure [S'])."""
+    atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    energy = np.ascontiguousarray(energy, dtype=np.float64)
+    forces = np.ascontiguousarray(forces, dtype=np.float64).reshape(-1, 3)
+    S = len(atom_off) - 1
+    N = int(atom_off[-1]) if S else 0
+    So, No = S * (1 + nadd), N * (1 + nadd)
+    oo = np.zeros(So + 1, dtype=np.int64)
+    op = np.zeros((max(No, 1), 3))
+    ot = np.zeros(max(No, 1), dtype=np.int32)
+    oe = np.zeros(max(So, 1))
+    osrc = np.zeros(max(So, 1), dtype=np.int32)
+    n = C.c_int32()
+    d = DISTRIBUTIONS.get(dist, dist) if isinstance(dist, str) else dist
+    rc = lib().nnp_taylor_expand(S, _ptr(atom_off), _ptr(pos), _ptr(types), _ptr(energy), _ptr(forces), int(nadd),
+                                 int(d) if not isinstance(d, str) else 0, float(rdelta), int(seed) & (2**64 - 1),
+                                 _ptr(oo), _ptr(op), _ptr(ot), _ptr(oe), _ptr(osrc), C.byref(n))
+    if rc != NNP_OK:
+        raise NNPError(rc, lib().nnp_last_error(None).decode())
+    k = n.value
+    na = int(oo[k])
+    return oo[:k + 1], op[:na], ot[:na], oe[:k], osrc[:k]

@@ -295,6 +295,25 @@ int nnp_input_stats(nnp_handle *h, const nnp_batch *batch, int64_t *count, doubl
 int nnp_precondition(nnp_handle *h, const nnp_batch *batch, int32_t prebias, int32_t prescale, double inbias,
                      double inscale);
 
+/* Taylor expansion of a training set (NNPTEFR's force perturbation,
+ * nnptefr.cpp:2733-2830), on the current CUDA device, no handle: each
+ * structure whose mean force norm exceeds 1e-12 is followed by nadd copies
+ * in which every atom j moves by dr_j = vr (sin t cos p, sin t sin p, cos t)
+ * (cos t, p / pi uniform in (-1, 1)) with vr drawn from distribution dist of
+ * width rdelta -- rng::dist::Name (math/random.hpp:32-42): 1 UNIFORM(0, w),
+ * 2 LAPLACE(0, w), 3 NORMAL(0, w), 5 SECH(0, w), 6 LOGISTIC(0, w), 7 COSINE(0, w)
+ * -- and whose energy is E - sum_j dr_j . F_j.  The random numbers are a
+ * counter-based hash of (seed, output structure, atom): the same inputs and
+ * seed give the same copies (the reference's std::mt19937 stream is not
+ * reproduced).  Host arrays.  Outputs hold up to n_struct * (1 + nadd)
+ * structures: out_atom_off[n_out+1], out_pos[3*atoms], out_type[atoms],
+ * out_energy[n_out], out_src[n_out] (the source structure of each, whose
+ * cell the caller reuses), *n_out.  Errors: nnp_last_error(NULL). */
+int nnp_taylor_expand(int32_t n_struct, const int64_t *atom_off, const double *pos, const int32_t *type,
+                      const double *energy, const double *forces, int32_t nadd, int32_t dist, double rdelta,
+                      uint64_t seed, int64_t *out_atom_off, double *out_pos, int32_t *out_type, double *out_energy,
+                      int32_t *out_src, int32_t *n_out);
+
 /* Energy-loss kind of nnp_train_grad, opt::Loss (opt/loss.hpp:18-24) as
  * NNPTEFR::error_cost_o1 applies it to dU = norm_s (E_s - e_ref_s)
  * (nnptefr.cpp:1340-1376): MSE 0.5 dU^2 (the default), MAE |dU|,
@@ -350,7 +369,8 @@ int nnp_neighbor_counts(nnp_handle *h, int32_t *counts);
 /* Kernels this handle has launched since it was created. */
 int nnp_launch_count(const nnp_handle *h, int64_t *n);
 
-/* Message of the last error on this handle (or of the last failed create when h is NULL). */
+/* Message of the last error on this handle (or, when h is NULL, of the last
+ * failed create or handle-free call such as nnp_taylor_expand). */
 const char *nnp_last_error(const nnp_handle *h);
 
 /* Library version string. */
