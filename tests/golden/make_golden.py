@@ -50,6 +50,44 @@ def cases():
     return out
 
 
+def make_large(name, k, b):
+    """A full-size fixture: the reference's energies and forces (no symmetry
+    functions, to keep the file small) of one large structure of
+    configuration k, potential conditioned as for the small fixtures."""
+    import tempfile
+    pot = synth.potential_config(k)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "pot.nnp")
+        potential.write(path, pot)
+        rp = ref.RefNNP(path)
+        cb = conditioning_batch(k)
+        G = np.concatenate([rp.compute(*cb.structure(s), want_symm=True)[3] for s in range(cb.n_struct)])
+        rp.close()
+        synth.condition(pot, G[:, :max(pot.n_input(t) for t in range(pot.ntypes))], cb.type)
+        potential.write(path, pot)
+        text = open(path).read()
+        rp = ref.RefNNP(path)
+        E, EV, F = [], [], []
+        for s in range(b.n_struct):
+            e, f, ev, _ = rp.compute(*b.structure(s))
+            E.append(e)
+            EV.append(ev)
+            F.append(f)
+        rp.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), potential=np.frombuffer(text.encode(), dtype=np.uint8),
+                        atom_off=b.atom_off, pos=b.pos, type=b.type, cell=np.asarray(b.cell).reshape(-1, 9),
+                        pbc=np.array(True), energy=np.array(E), energy_vacuum=np.array(EV),
+                        forces=np.concatenate(F), config=np.array(k))
+
+
+def large_cases():
+    """Configuration 4's jittered FCC lattice at 10^3 cells (4000 atoms,
+    rc 6.5 A) and one 2048-atom structure of configuration 5's generator."""
+    rng = np.random.default_rng(705)
+    return [("large_config4", 4, synth.config4(seed=704, ncell=10)),
+            ("large_config5", 5, synth.batch_random(705, [2048], 4))]
+
+
 def form_cases():
     """(name, batch) of the fixtures of the other basis forms, cutoffs and
     activations (synth.FORM_POTENTIALS): 4 periodic structures of 8-48 atoms."""
@@ -238,6 +276,11 @@ if __name__ == "__main__":
         if which and name not in which:
             continue
         make_forms(name, b)
+        print("wrote", name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
+    for name, k, b in large_cases():
+        if which and name not in which:
+            continue
+        make_large(name, k, b)
         print("wrote", name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
     if not which or "train_config3" in which:
         make_train()

@@ -248,11 +248,18 @@ def test_compute_energy_from_symm(tmp_path):
 
 def test_full_size_properties(tmp_path):
     """Config-2-sized batch: momentum conservation (sum of forces per structure
-    vanishes) and invariance of energies under a rigid shift + lattice wrap."""
+    vanishes), invariance of energies under a rigid shift + lattice wrap, and
+    energies and forces of six sampled structures against the oracle."""
     b = synth.config2(n_struct=512)
     path = make_pot(tmp_path, 2, b.subset(range(8)))
     nn = NNP.read(path)
     E, F = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
+    op = orc.OraclePot.from_file(path)
+    for s in (0, 101, 202, 303, 404, 511):
+        a0, a1 = b.atom_off[s], b.atom_off[s + 1]
+        eo, fo, _ = orc.compute(op, *b.structure(s))
+        assert abs(E[s] - eo) / (a1 - a0) < E_ATOL
+        assert np.abs(F[a0:a1] - fo).max() < F_ATOL
     for s in range(0, b.n_struct, 37):
         fs = F[b.atom_off[s]:b.atom_off[s + 1]]
         assert np.abs(fs.sum(axis=0)).max() < 1e-4 * max(1.0, np.abs(fs).max())
