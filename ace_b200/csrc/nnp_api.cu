@@ -71,6 +71,7 @@ void Engine::free_all()
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();
+    adam_idx.release(); adam_p.release(); adam_m.release(); adam_v.release();
     graph_release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
@@ -230,6 +231,7 @@ std::string Engine::upload()
 {
     std::string msg = build_tables();
     if (!msg.empty()) return msg;
+    adam_master_stale = true;
     const DevPot &d = dpot;
     std::vector<float2> rp = rpar_host;
     std::vector<float4> ap = apar_host;
@@ -1146,6 +1148,95 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
     return NNP_OK;
 }
 
+int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
+{
+    if (!h) return NNP_ERR_ARG;
+    nnp::Engine &E = h->E;
+    if (!E.grad_valid) return fail(h, NNP_ERR_ARG, "no gradient: call nnp_train_grad first");
+    if (!(gamma >= 0.0) || !std::isfinite(gamma)) return fail(h, NNP_ERR_ARG, "gamma must be finite and non-negative");
+    if (eps < 0.0 || eps > 1.0) return fail(h, NNP_ERR_ARG, "opt::algo::ADAM::read(Token&): Invalid eps.");
+    cudaError_t ce = cudaSuccess;
+    auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
+    if (E.adam_master_stale) {
+        // parameters in the reference packing: their wpar offsets and FP64 values
+        std::vector<int64_t> idx;
+        std::vector<double> val;
+        for (int t = 0; t < E.dpot.ntypes; ++t) {
+            const nnp::DevType &T = E.dpot.t[t];
+            const nnp::HostNet &net = E.host.nets[t];
+            const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+            int64_t off = T.woff + 2 * nin + 2 * nout;
+            std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
+            for (int l = 0; l < T.nlayer; ++l) {
+                boff[l] = off;
+                woff[l] = off + T.nodes[l + 1];
+                off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
+            }
+            for (int l = 0; l < T.nlayer; ++l)
+                for (int n = 0; n < T.nodes[l + 1]; ++n) {
+                    idx.push_back(boff[l] + n);
+                    val.push_back(net.b[l][n]);
+                }
+            for (int l = 0; l < T.nlayer; ++l) {
+                const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
+                for (int m = 0; m < ni; ++m)
+                    for (int n = 0; n < no; ++n) {
+                        idx.push_back(woff[l] + (int64_t)m * st + n);
+                        val.push_back(net.w[l][(size_t)n * ni + m]);
+                    }
+            }
+        }
+        const bool fresh = E.adam_idx_host.size() != idx.size();
+        E.adam_idx_host = idx;
+        const size_t n = idx.size();
+        chk(E.adam_idx.reserve(n));
+        chk(E.adam_p.reserve(n));
+        chk(E.adam_m.reserve(n));
+        chk(E.adam_v.reserve(n));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
+        chk(cudaMemcpyAsync(E.adam_idx.p, idx.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, E.stream));
+        chk(cudaMemcpyAsync(E.adam_p.p, val.data(), sizeof(double) * n, cudaMemcpyHostToDevice, E.stream));
+        if (fresh) {        // first step (ADAM::resize): zero averages, powers beta^1
+            chk(cudaMemsetAsync(E.adam_m.p, 0, sizeof(double) * n, E.stream));
+            chk(cudaMemsetAsync(E.adam_v.p, 0, sizeof(double) * n, E.stream));
+            E.adam_b1i = 0.9;
+            E.adam_b2i = 0.999;
+        }
+        chk(cudaStreamSynchronize(E.stream));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("ADAM set-up failed: ") + cudaGetErrorString(ce));
+        E.adam_master_stale = false;
+    }
+    std::string msg = nnp::run_adam(E, gamma, eps);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    // mirror the new parameters into the host model (nnp_get_params, nnp_write)
+    std::vector<double> val(E.adam_idx_host.size());
+    chk(cudaMemcpyAsync(val.data(), E.adam_p.p, sizeof(double) * val.size(), cudaMemcpyDeviceToHost, E.stream));
+    chk(cudaStreamSynchronize(E.stream));
+    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("ADAM step failed: ") + cudaGetErrorString(ce));
+    size_t k = 0;
+    for (auto &net : E.host.nets) {
+        const int nl = (int)net.nodes.size() - 1;
+        for (int l = 0; l < nl; ++l)
+            for (auto &v : net.b[l]) v = val[k++];
+        for (int l = 0; l < nl; ++l) {
+            const int ni = net.nodes[l], no = net.nodes[l + 1];
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) net.w[l][(size_t)n * ni + m] = val[k++];
+        }
+    }
+    for (size_t i = 0; i < E.adam_idx_host.size(); ++i) E.wpar_host[E.adam_idx_host[i]] = (float)val[i];
+    E.grad_valid = false;
+    return NNP_OK;
+}
+
+int nnp_opt_reset(nnp_handle *h)
+{
+    if (!h) return NNP_ERR_ARG;
+    h->E.adam_idx_host.clear();
+    h->E.adam_master_stale = true;
+    return NNP_OK;
+}
+
 int nnp_set_mma_wait(nnp_handle *h, int64_t polls)
 {
     if (!h) return NNP_ERR_ARG;
@@ -1313,8 +1404,10 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, c
     chk(cudaMemcpyAsync(E.gE.p, ge.data(), sizeof(float) * N, cudaMemcpyHostToDevice, E.stream));
     if (w_f != 0.0) chk(cudaMemcpyAsync(E.tvec.p, tv.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
     if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("copy failed: ") + cudaGetErrorString(ce));
+    E.grad_valid = false;
     std::string msg = nnp::run_train_grad(E, w_f != 0.0);
     if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    E.grad_valid = true;
     std::vector<double> gw((size_t)E.wfloats);
     chk(cudaMemcpyAsync(gw.data(), E.pgrad.p, sizeof(double) * E.wfloats, cudaMemcpyDeviceToHost, E.stream));
     chk(cudaStreamSynchronize(E.stream));

@@ -221,3 +221,45 @@ std::string run_train_grad(Engine &E, bool with_force)
 }
 
 }  // namespace nnp
+
+namespace nnp {
+
+// One ADAM step (opt::algo::ADAM::step, opt/algo.cpp:280-296) over the n
+// network parameters, with the gradient of the last training call still on
+// the device (grad, wpar layout, at idx[i]): running averages m, v of the
+// gradient and its square, p -= gamma b1ii m / (sqrt(b2ii v) + eps) on the
+// FP64 master copy p64, and its FP32 value written into the networks' table.
+__global__ void k_adam(int64_t n, const int64_t *__restrict__ idx, const double *__restrict__ grad,
+                       double *__restrict__ p64, double *__restrict__ m, double *__restrict__ v,
+                       float *__restrict__ wpar, double gamma, double b1ii, double b2ii, double eps)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    constexpr double beta1 = 0.9, beta2 = 0.999;
+    const double g = grad[idx[i]];
+    double mm = m[i], vv = v[i];
+    mm *= beta1;
+    mm += (1.0 - beta1) * g;
+    vv *= beta2;
+    vv += (1.0 - beta2) * g * g;
+    m[i] = mm;
+    v[i] = vv;
+    const double p = p64[i] - gamma * b1ii * mm / (sqrt(b2ii * vv) + eps);
+    p64[i] = p;
+    wpar[idx[i]] = (float)p;
+}
+
+std::string run_adam(Engine &E, double gamma, double eps)
+{
+    const int64_t n = (int64_t)E.adam_idx_host.size();
+    if (n == 0) return "";
+    const double b1ii = 1.0 / (1.0 - E.adam_b1i), b2ii = 1.0 / (1.0 - E.adam_b2i);
+    k_adam<<<(int)((n + 255) / 256), 256, 0, E.stream>>>(n, E.adam_idx.p, E.pgrad.p, E.adam_p.p, E.adam_m.p,
+                                                           E.adam_v.p, E.wpar.p, gamma, b1ii, b2ii, eps);
+    E.launches += 1;
+    E.adam_b1i *= 0.9;
+    E.adam_b2i *= 0.999;
+    return cuda_msg("ADAM step");
+}
+
+}  // namespace nnp

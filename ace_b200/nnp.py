@@ -76,6 +76,8 @@ def lib():
             "nnp_set_params": ([p, p], i),
             "nnp_train_grad": ([p, C.POINTER(_Batch), p, p, d, i, p, p, p, p, u], i),
             "nnp_set_loss": ([p, i, d], i),
+            "nnp_opt_adam": ([p, d, d], i),
+            "nnp_opt_reset": ([p], i),
             "nnp_set_mma_wait": ([p, C.c_int64], i),
             "nnp_set_autotune": ([p, i], i),
             "nnp_tune_params": ([p, p, i, C.POINTER(i), C.POINTER(C.c_char_p)], i),
@@ -190,6 +192,13 @@ class NNP:
         """Energy-loss kind of train_grad (LOSS_MSE, LOSS_MAE, LOSS_HUBER,
         LOSS_ASINH) and its width, as nnptefr's loss / delta settings."""
         self._check(lib().nnp_set_loss(self._h, kind, float(delta)))
+
+    def opt_adam(self, gamma: float, eps: float = 1e-16):
+        """One ADAM step on the device with the last train_grad gradient."""
+        self._check(lib().nnp_opt_adam(self._h, float(gamma), float(eps)))
+
+    def opt_reset(self):
+        self._check(lib().nnp_opt_reset(self._h))
 
     def set_mma_wait(self, polls: int):
         """Bound of each tensor-core MMA-chain wait (0: the default)."""

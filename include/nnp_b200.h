@@ -327,6 +327,19 @@ int nnp_taylor_expand(int32_t n_struct, const int64_t *atom_off, const double *p
 #define NNP_LOSS_ASINH 4
 int nnp_set_loss(nnp_handle *h, int32_t kind, double delta);
 
+/* One ADAM step on the device (opt::algo::ADAM::step, opt/algo.cpp:280-296,
+ * beta1 0.9, beta2 0.999) with the gradient of the last nnp_train_grad,
+ * which stays on the device: m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
+ * p -= gamma m / (1 - b1^t) / (sqrt(v / (1 - b2^t)) + eps).  The running
+ * averages and an FP64 master copy of the parameters live on the handle
+ * (zeroed at the first step, as ADAM::resize); the networks the next call
+ * uses are updated on the device, and the host model (nnp_get_params,
+ * nnp_write) is updated with them.  The learning rate gamma is the caller's
+ * (the reference's decay schedules set it per step).  nnp_opt_reset
+ * restarts the averages.  nnptefr's binary restart file is not read or written. */
+int nnp_opt_adam(nnp_handle *h, double gamma, double eps);
+int nnp_opt_reset(nnp_handle *h);
+
 /* Allocation-free energies from device-resident symmetry functions (no
  * counterpart in the reference, whose NNP::compute_energy (nnp.cpp:329-338)
  * it otherwise follows).  For callers that must not allocate device memory
