@@ -896,6 +896,60 @@ int nnp_compute_md(nnp_handle *h, const nnp_batch *b, double *energy, double *fo
     return compute_impl(h, b, energy, forces, nullptr, atom_energy, virial, flags);
 }
 
+int nnp_type_name(const nnp_handle *h, int32_t type, const char **name)
+{
+    if (!h || !name || type < 0 || type >= h->E.host.ntypes()) return NNP_ERR_ARG;
+    *name = h->E.host.types[type].name.c_str();
+    return NNP_OK;
+}
+
+int nnp_read_structures(int32_t ntypes, const char *const *type_names, const char *path, int32_t format,
+                        int32_t *n_struct, int64_t *n_atoms, int64_t *atom_off, double *pos, int32_t *type,
+                        double *cell, int32_t *pbc, double *energy, double *forces)
+{
+    auto bad = [](int code, const std::string &m) {
+        g_create_error = m;
+        return code;
+    };
+    if (ntypes < 0 || (ntypes > 0 && !type_names) || !path || !n_struct || !n_atoms) return bad(NNP_ERR_ARG, "bad argument");
+    if (format != NNP_FMT_XYZ && format != NNP_FMT_VASP) return bad(NNP_ERR_ARG, "unknown structure format");
+    std::string text;
+    if (!read_file(path, text)) return bad(NNP_ERR_IO, std::string("Could not open file: ") + path);
+    std::vector<nnp::ReadStruct> rs;
+    const std::string msg = format == NNP_FMT_XYZ ? nnp::read_xyz_frames(text, rs) : nnp::read_vasp(text, rs);
+    if (!msg.empty()) return bad(NNP_ERR_PARSE, msg);
+    int64_t N = 0;
+    for (const auto &r : rs) N += (int64_t)r.names.size();
+    if (atom_off) {
+        if (*n_struct < (int32_t)rs.size() || *n_atoms < N)
+            return bad(NNP_ERR_CAPACITY, "output arrays hold fewer structures or atoms than the file");
+        int64_t a = 0;
+        atom_off[0] = 0;
+        for (size_t s = 0; s < rs.size(); ++s) {
+            const nnp::ReadStruct &r = rs[s];
+            for (size_t i = 0; i < r.names.size(); ++i, ++a) {
+                int t = -1;
+                for (int k = 0; k < ntypes; ++k)
+                    if (type_names[k] && r.names[i] == type_names[k]) t = k;
+                if (t < 0) return bad(NNP_ERR_TYPE, "element \"" + r.names[i] + "\" is not in the potential");
+                if (type) type[a] = t;
+                if (pos)
+                    for (int d = 0; d < 3; ++d) pos[3 * a + d] = r.pos[3 * i + d];
+                if (forces)
+                    for (int d = 0; d < 3; ++d) forces[3 * a + d] = r.forces[3 * i + d];
+            }
+            atom_off[s + 1] = a;
+            if (cell)
+                for (int k = 0; k < 9; ++k) cell[9 * s + k] = r.cell[k];
+            if (pbc) pbc[s] = r.pbc ? 1 : 0;
+            if (energy) energy[s] = r.energy;
+        }
+    }
+    *n_struct = (int32_t)rs.size();
+    *n_atoms = N;
+    return NNP_OK;
+}
+
 int nnp_input_stats(nnp_handle *h, const nnp_batch *batch, int64_t *count, double *stats)
 {
     if (!h || !batch || !count || !stats) return NNP_ERR_ARG;

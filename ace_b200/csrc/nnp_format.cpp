@@ -7,6 +7,8 @@
 // "basis_angular Y Z" + BasisA block per pair Y<=Z (basis_angular.cpp:116-138),
 // then per type "nn X" followed by an ANN block (ml/nn.cpp:1536-1613).
 // write_potential reproduces NNP::write (nnp.cpp:197-236) byte for byte.
+#include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -390,6 +392,186 @@ std::string write_potential(const HostPot &pot)
         }
     }
     return s;
+}
+
+}  // namespace nnp
+
+// ------------------------------------------------------------------ structure files
+//
+// Readers of the structure formats the reference's training and test
+// programs take (format/xyz_struc.cpp, format/vasp_struc.cpp), into the CSR
+// batch of the C ABI, in the reference's METAL units (A, eV).
+
+namespace nnp {
+
+namespace {
+
+std::vector<std::string> split_ws(const std::string &s)
+{
+    std::vector<std::string> out;
+    std::istringstream is(s);
+    std::string t;
+    while (is >> t) out.push_back(t);
+    return out;
+}
+
+// value text after "KEY=" in an extended-XYZ comment line (quotes removed)
+bool xyz_field(const std::string &line, const std::string &key, std::string &val)
+{
+    const std::string up = upper(line);
+    const size_t k = up.find(key);
+    if (k == std::string::npos) return false;
+    size_t p = k + key.size();
+    while (p < line.size() && (line[p] == ' ' || line[p] == '=' || line[p] == '\t')) ++p;
+    if (p < line.size() && line[p] == '"') {
+        const size_t e = line.find('"', p + 1);
+        val = line.substr(p + 1, e == std::string::npos ? std::string::npos : e - p - 1);
+    } else {
+        size_t e = p;
+        while (e < line.size() && !std::isspace((unsigned char)line[e])) ++e;
+        val = line.substr(p, e - p);
+    }
+    return true;
+}
+
+// positions back into the cell, Cell::returnToCell (struc/cell.cpp): fractional
+// coordinates reduced to [0, 1)
+void wrap_into_cell(const double R[9], double *x)
+{
+    // R[3n + d] = component d of lattice vector n; solve R q = x
+    const double *a = R, *b = R + 3, *c = R + 6;
+    const double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+    const double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+    const double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    const double V = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+    if (!(std::fabs(V) > 0)) return;
+    double q[3] = {(bc[0] * x[0] + bc[1] * x[1] + bc[2] * x[2]) / V, (ca[0] * x[0] + ca[1] * x[1] + ca[2] * x[2]) / V,
+                   (ab[0] * x[0] + ab[1] * x[1] + ab[2] * x[2]) / V};
+    for (double &v : q) v -= std::floor(v);
+    for (int d = 0; d < 3; ++d) x[d] = R[d] * q[0] + R[3 + d] * q[1] + R[6 + d] * q[2];
+}
+
+}  // namespace
+
+// Extended XYZ (every frame of the file): line 1 the atom count, line 2
+// Properties=species:S:1:pos:R:3[:forces:R:3...], potential_energy=E and
+// Lattice="a1 a2 a3" (vectors in turn), then one line per atom
+// (XYZ::read, format/xyz_struc.cpp:26-180).  Without a Properties field the
+// atom lines are "name x y z".  A frame with a lattice is periodic and its
+// positions are wrapped into the cell, as the reference does.
+std::string read_xyz_frames(const std::string &text, std::vector<ReadStruct> &out)
+{
+    std::istringstream in(text);
+    std::string line;
+    while (std::getline(in, line)) {
+        const std::vector<std::string> t0 = split_ws(line);
+        if (t0.empty()) continue;
+        char *end = nullptr;
+        const long n = std::strtol(t0[0].c_str(), &end, 10);
+        if (!end || *end || n <= 0) return "XYZ: expected an atom count, found \"" + line + "\"";
+        std::string head;
+        if (!std::getline(in, head)) return "XYZ: missing comment line";
+        ReadStruct rs;
+        rs.pbc = false;
+        rs.energy = 0.0;
+        std::fill(rs.cell, rs.cell + 9, 0.0);
+        // columns of the atom lines
+        int ndata = 0, ni = 0, ri = 1, fi = -1;
+        std::string props;
+        if (xyz_field(head, "PROPERTIES", props)) {
+            ni = ri = -1;
+            std::vector<std::string> f;
+            std::string cur;
+            for (char c : props) {
+                if (c == ':') { f.push_back(cur); cur.clear(); }
+                else cur += c;
+            }
+            f.push_back(cur);
+            for (size_t k = 0; k + 2 < f.size(); k += 3) {
+                const std::string tag = upper(f[k]);
+                const int len = std::atoi(f[k + 2].c_str());
+                if (tag == "SPECIES") ni = ndata;
+                else if (tag == "POS" || tag == "POSN" || tag == "POSITION") ri = ndata;
+                else if (tag == "FORCES" || tag == "FORCE") fi = ndata;
+                ndata += len;
+            }
+            if (ni < 0 || ri < 0) return "XYZ: Properties without species and positions";
+        }
+        std::string v;
+        if (xyz_field(head, "POTENTIAL_ENERGY", v)) rs.energy = std::atof(v.c_str());
+        if (xyz_field(head, "LATTICE", v)) {
+            const std::vector<std::string> L = split_ws(v);
+            if (L.size() != 9) return "XYZ: Lattice needs 9 numbers";
+            double nrm = 0;
+            for (int k = 0; k < 9; ++k) {
+                rs.cell[k] = std::atof(L[k].c_str());
+                nrm += rs.cell[k] * rs.cell[k];
+            }
+            rs.pbc = nrm > 0;
+        }
+        rs.has_forces = fi >= 0;
+        for (long i = 0; i < n; ++i) {
+            if (!std::getline(in, line)) return "XYZ: fewer atom lines than the atom count";
+            const std::vector<std::string> a = split_ws(line);
+            const int need = std::max({ni + 1, ri + 3, fi >= 0 ? fi + 3 : 0});
+            if ((int)a.size() < need) return "XYZ: short atom line \"" + line + "\"";
+            rs.names.push_back(a[ni]);
+            double x[3] = {std::atof(a[ri].c_str()), std::atof(a[ri + 1].c_str()), std::atof(a[ri + 2].c_str())};
+            if (rs.pbc) wrap_into_cell(rs.cell, x);
+            rs.pos.insert(rs.pos.end(), x, x + 3);
+            for (int d = 0; d < 3; ++d) rs.forces.push_back(fi >= 0 ? std::atof(a[fi + d].c_str()) : 0.0);
+        }
+        out.push_back(std::move(rs));
+    }
+    return "";
+}
+
+// VASP POSCAR / CONTCAR (VASP::POSCAR::read, format/vasp_struc.cpp:41-190): comment,
+// scale, three lattice vectors (times the scale), species names, counts,
+// "Direct" or Cartesian, positions.  As in the reference, Cartesian positions
+// are taken as they stand (the scale multiplies the lattice only).
+std::string read_vasp(const std::string &text, std::vector<ReadStruct> &out)
+{
+    std::istringstream in(text);
+    std::string line;
+    auto next = [&](std::string &l) { return (bool)std::getline(in, l); };
+    ReadStruct rs;
+    if (!next(line)) return "VASP: empty file";
+    if (!next(line)) return "VASP: missing scale";
+    const double scale = std::atof(line.c_str());
+    for (int n = 0; n < 3; ++n) {
+        if (!next(line)) return "VASP: missing lattice vector";
+        const std::vector<std::string> v = split_ws(line);
+        if (v.size() < 3) return "VASP: short lattice vector";
+        for (int d = 0; d < 3; ++d) rs.cell[3 * n + d] = std::atof(v[d].c_str()) * scale;
+    }
+    std::string sn, sc;
+    if (!next(sn) || !next(sc)) return "VASP: missing species";
+    const std::vector<std::string> names = split_ws(sn), counts = split_ws(sc);
+    if (names.empty() || names.size() != counts.size()) return "Invalid number of species";
+    if (!next(line)) return "VASP: missing coordinate mode";
+    const bool direct = !line.empty() && line[0] == 'D';
+    for (size_t s = 0; s < names.size(); ++s) {
+        const int c = std::atoi(counts[s].c_str());
+        for (int m = 0; m < c; ++m) {
+            if (!next(line)) return "VASP: fewer positions than atoms";
+            const std::vector<std::string> v = split_ws(line);
+            if (v.size() < 3) return "VASP: short position line";
+            double x[3] = {std::atof(v[0].c_str()), std::atof(v[1].c_str()), std::atof(v[2].c_str())};
+            if (direct) {
+                const double q[3] = {x[0], x[1], x[2]};
+                for (int d = 0; d < 3; ++d) x[d] = rs.cell[d] * q[0] + rs.cell[3 + d] * q[1] + rs.cell[6 + d] * q[2];
+            }
+            rs.pos.insert(rs.pos.end(), x, x + 3);
+            rs.names.push_back(names[s]);
+            for (int d = 0; d < 3; ++d) rs.forces.push_back(0.0);
+        }
+    }
+    rs.pbc = true;
+    rs.energy = 0.0;
+    rs.has_forces = false;
+    out.push_back(std::move(rs));
+    return "";
 }
 
 }  // namespace nnp

@@ -44,6 +44,18 @@ std::string write_potential(const HostPot &pot);
 std::string read_basis_file(const std::string &text, HostPot &pot, int II);
 std::string read_network(const std::string &text, HostNet &net);
 
+// One structure read from a structure file (nnp_read_structures).
+struct ReadStruct {
+    std::vector<std::string> names;   // element of each atom
+    std::vector<double> pos;          // 3 per atom, A
+    std::vector<double> forces;       // 3 per atom, eV/A (zero when the file has none)
+    double cell[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // cell[3n+d]: component d of lattice vector n
+    double energy = 0;                // potential energy, eV
+    bool pbc = false, has_forces = false;
+};
+std::string read_xyz_frames(const std::string &text, std::vector<ReadStruct> &out);
+std::string read_vasp(const std::string &text, std::vector<ReadStruct> &out);
+
 // A network's floats in wpar, starting at DevType::woff:
 //   inpw[nin], inpb[nin], outw[nout], outb[nout],
 //   then for each layer l: bias[no] and the weights transposed with a padded

@@ -67,6 +67,8 @@ def lib():
             "nnp_compute_md": ([p, C.POINTER(_Batch), p, p, p, p, u], i),
             "nnp_compute_local_ghost": ([p, C.c_int64, C.c_int64, p, p, p, p, p, p, u], i),
             "nnp_input_stats": ([p, C.POINTER(_Batch), p, p], i),
+            "nnp_read_structures": ([i, p, C.c_char_p, i, C.POINTER(i), C.POINTER(C.c_int64), p, p, p, p, p, p, p], i),
+            "nnp_type_name": ([p, i, C.POINTER(C.c_char_p)], i),
             "nnp_taylor_expand": ([i, p, p, p, p, p, i, i, d, C.c_uint64, p, p, p, p, p, C.POINTER(i)], i),
             "nnp_precondition": ([p, C.POINTER(_Batch), i, i, d, d], i),
             "nnp_set_graphs": ([p, i], i),
@@ -203,6 +205,18 @@ class NNP:
     def set_mma_wait(self, polls: int):
         """Bound of each tensor-core MMA-chain wait (0: the default)."""
         self._check(lib().nnp_set_mma_wait(self._h, int(polls)))
+
+    def type_names(self):
+        out = []
+        for t in range(self.ntypes):
+            v = C.c_char_p()
+            self._check(lib().nnp_type_name(self._h, t, C.byref(v)))
+            out.append(v.value.decode())
+        return out
+
+    def read_structures(self, path: str, fmt: str = "xyz"):
+        """read_structures with this potential's element names."""
+        return read_structures(path, self.type_names(), fmt)
 
     def _batch(self, atom_off, pos, types, cells, pbc):
         atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
@@ -480,3 +494,30 @@ def taylor_expand(atom_off, pos, types, energy, forces, nadd, dist="NORMAL", rde
     k = n.value
     na = int(oo[k])
     return oo[:k + 1], op[:na], ot[:na], oe[:k], osrc[:k]
+
+
+def read_structures(path: str, type_names, fmt: str = "xyz"):
+    """Structures of an extended-XYZ or VASP file as a CSR batch (host only):
+    (atom_off, pos [N,3], types [N], cells [S,3,3] (vectors as rows),
+    pbc [S], energies [S], forces [N,3])."""
+    code = {"xyz": 1, "vasp": 2}[fmt.lower()]
+    T = len(type_names)
+    names = (C.c_char_p * max(T, 1))(*[n.encode() for n in type_names])
+    ns, na = C.c_int32(), C.c_int64()
+    rc = lib().nnp_read_structures(T, C.cast(names, C.c_void_p), os.fsencode(path), code, C.byref(ns), C.byref(na),
+                                   None, None, None, None, None, None, None)
+    if rc != NNP_OK:
+        raise NNPError(rc, lib().nnp_last_error(None).decode())
+    S, N = ns.value, na.value
+    off = np.zeros(S + 1, dtype=np.int64)
+    pos = np.zeros((max(N, 1), 3))
+    typ = np.zeros(max(N, 1), dtype=np.int32)
+    cell = np.zeros((max(S, 1), 3, 3))
+    pbc = np.zeros(max(S, 1), dtype=np.int32)
+    en = np.zeros(max(S, 1))
+    frc = np.zeros((max(N, 1), 3))
+    rc = lib().nnp_read_structures(T, C.cast(names, C.c_void_p), os.fsencode(path), code, C.byref(ns), C.byref(na),
+                                   _ptr(off), _ptr(pos), _ptr(typ), _ptr(cell), _ptr(pbc), _ptr(en), _ptr(frc))
+    if rc != NNP_OK:
+        raise NNPError(rc, lib().nnp_last_error(None).decode())
+    return off, pos[:N], typ[:N], cell[:S], pbc[:S].astype(bool), en[:S], frc[:N]

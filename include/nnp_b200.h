@@ -253,6 +253,31 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);
 
+/* Structure files into a CSR batch: extended XYZ, every frame of the file
+ * (XYZ::read, format/xyz_struc.cpp:26-180: Properties=species:S:1:pos:R:3
+ * [:forces:R:3], potential_energy=, Lattice="a1 a2 a3"; plain "name x y z"
+ * lines when there is no Properties field; positions of a periodic frame
+ * wrapped into its cell), or a VASP POSCAR/CONTCAR, one structure
+ * (VASP::POSCAR::read, format/vasp_struc.cpp:41-190; as in the reference the scale
+ * multiplies the lattice, not Cartesian positions).  METAL units (A, eV).
+ * Element names are mapped to type indices by type_names[ntypes] (a
+ * potential's names in index order, nnp_type_name; NNP::index); an unknown
+ * name is NNP_ERR_TYPE.  Host only, no handle or GPU; errors in
+ * nnp_last_error(NULL).  Call with atom_off = NULL to get the sizes
+ * (*n_struct, *n_atoms); then with arrays of at least those sizes (in:
+ * capacities, out: sizes): atom_off[n_struct+1], pos[3N], type[N],
+ * cell[9 n_struct], pbc[n_struct] (1 when the frame has a lattice),
+ * energy[n_struct] (0 when the file has none), forces[3N] (0 when none);
+ * any of the last six may be NULL. */
+#define NNP_FMT_XYZ 1
+#define NNP_FMT_VASP 2
+int nnp_read_structures(int32_t ntypes, const char *const *type_names, const char *path, int32_t format,
+                        int32_t *n_struct, int64_t *n_atoms, int64_t *atom_off, double *pos, int32_t *type,
+                        double *cell, int32_t *pbc, double *energy, double *forces);
+
+/* Name of element `type` of the potential (NNP::nnh(type).type().name()). */
+int nnp_type_name(const nnp_handle *h, int32_t type, const char **name);
+
 /* Input statistics of the networks over a training set: NNPTEFR::train's
  * statistics of the symmetry functions per element (nnptefr.cpp:689-781),
  * computed on the device from the batch's symmetry functions (the

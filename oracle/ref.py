@@ -37,6 +37,8 @@ def lib():
         L.ref_nnp_compute.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, C.c_int, dp, dp, dp, dp,
                                       C.c_char_p, C.c_int]
         L.ref_nnp_nparams.argtypes = [p, C.c_int]
+        L.ref_read_structure.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp, dp, dp,
+                                         C.c_char_p, C.c_int, C.c_char_p, C.c_int]
         L.ref_energy_loss_grad.argtypes = [p, C.c_int, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int), dp, C.c_int,
                                            dp, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, C.c_char_p, C.c_int]
         L.ref_force_term_grad.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, dp, C.c_double, dp,
@@ -137,3 +139,22 @@ class RefNNP:
         if rc != 0:
             raise RuntimeError("reference force-term gradient failed: " + err.value.decode())
         return (g, ct) if want_tangent else g
+
+
+def read_structure(path: str, fmt: str = "xyz", cap: int = 100000):
+    """One structure through the reference's XYZ::read / VASP::POSCAR::read:
+    (names, positions [n,3], forces [n,3], pe, cell [3,3] with the lattice
+    vectors as rows)."""
+    n = C.c_int()
+    pos = np.zeros((cap, 3))
+    frc = np.zeros((cap, 3))
+    pe = np.zeros(1)
+    cell = np.zeros(9)
+    names = C.create_string_buffer(16 * cap + 16)
+    err = C.create_string_buffer(512)
+    rc = lib().ref_read_structure(os.fsencode(path), 1 if fmt == "xyz" else 2, cap, C.byref(n), _dp(pos), _dp(frc),
+                                  _dp(pe), _dp(cell), names, len(names), err, len(err))
+    if rc != 0:
+        raise RuntimeError("reference read failed: " + err.value.decode())
+    k = n.value
+    return names.value.decode().split(), pos[:k], frc[:k], float(pe[0]), cell.reshape(3, 3)

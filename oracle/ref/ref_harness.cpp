@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include "format/vasp_struc.hpp"
+#include "format/xyz_struc.hpp"
 #include "ml/nn.hpp"
 #include "nnp/nnp.hpp"
 #include "struc/neighbor.hpp"
@@ -270,6 +272,43 @@ int ref_force_term_grad(void *h, int n, const double *pos, const int *type, cons
                 grad[off[t] + p] += s;
             }
         }
+        return 0;
+    } catch (std::exception &e) {
+        put(err, errlen, e.what());
+    }
+    return -1;
+}
+
+// One structure file through the reference's own reader: format 1 extended
+// XYZ (XYZ::read, first frame), 2 VASP POSCAR (VASP::read).  Writes the atom
+// count, positions[3n], forces[3n], pe, the lattice vectors cell[3c+d]
+// (zero without a cell) and the element names, one per line, into names.
+int ref_read_structure(const char *path, int format, int cap, int *n, double *pos, double *forces, double *pe,
+                       double *cell, char *names, int names_len, char *err, int errlen)
+{
+    try {
+        Atom atom;
+        atom.name() = true;
+        atom.type() = true;
+        atom.posn() = true;
+        atom.force() = true;
+        Structure struc;
+        if (format == 1) XYZ::read(path, atom, struc);
+        else VASP::POSCAR::read(path, atom, struc);
+        *n = struc.nAtoms();
+        if (struc.nAtoms() > cap) throw std::runtime_error("too many atoms");
+        for (int i = 0; i < struc.nAtoms(); ++i)
+            for (int d = 0; d < 3; ++d) {
+                pos[3 * i + d] = struc.posn(i)[d];
+                forces[3 * i + d] = format == 1 ? struc.force(i)[d] : 0.0;
+            }
+        *pe = struc.pe();
+        const Eigen::Matrix3d R = struc.R();
+        for (int c = 0; c < 3; ++c)
+            for (int d = 0; d < 3; ++d) cell[3 * c + d] = R(d, c);
+        std::string all;
+        for (int i = 0; i < struc.nAtoms(); ++i) all += struc.name(i) + "\n";
+        put(names, names_len, all);
         return 0;
     } catch (std::exception &e) {
         put(err, errlen, e.what());
