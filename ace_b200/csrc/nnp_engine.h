@@ -144,6 +144,7 @@ struct Engine {
     bool adam_master_stale = true;  // the master copy must be reloaded from the host model
     int loss_kind = 1;            // energy-loss kind of nnp_train_grad (NNP_LOSS_*)
     double loss_delta = 1.0;      // its width (HUBER, ASINH)
+    float *noalloc_e_atom = nullptr;  // device address of the allocation-free call's scratch (looked up once)
     DevErr *h_err = nullptr;      // pinned
     // pinned staging for host-pointer calls
     void *h_stage = nullptr;

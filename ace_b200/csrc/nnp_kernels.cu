@@ -1379,25 +1379,20 @@ __global__ void k_energy_noalloc(const int64_t *__restrict__ off, int64_t N, con
     if (threadIdx.x == 0) e_struct[s] = part[0];
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress may load the module; it allocates nothing
-// the caller owns).
-std::string noalloc_scratch(float **out)
+// Device address of the scratch array on the handle's device, looked up on
+// the handle's first allocation-free call (cudaGetSymbolAddress may load the
+// module; it allocates nothing the caller owns) and kept with the handle: a
+// handle lives in one CUDA context, so the address cannot go stale under it
+// (a handle made after a device reset looks it up again).
+std::string noalloc_scratch(Engine &E, float **out)
 {
-    static std::mutex mu;
-    static float *addr[256] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-    if (dev < 0 || dev >= 256) return "device ordinal out of range";
-    std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    if (!E.noalloc_e_atom) {
         float *p = nullptr;
-        e = cudaGetSymbolAddress((void **)&p, g_noalloc_e_atom);
+        const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_e_atom);
         if (e != cudaSuccess) return std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-        addr[dev] = p;
+        E.noalloc_e_atom = p;
     }
-    *out = addr[dev];
+    *out = E.noalloc_e_atom;
     return "";
 }
 
@@ -1405,7 +1400,7 @@ std::string run_energy_symm_noalloc(Engine &E, int S, int64_t N, const int64_t *
                                     const float *G, int gstride, bool vacuum, double *energy)
 {
     float *e_atom = nullptr;
-    std::string msg = noalloc_scratch(&e_atom);
+    std::string msg = noalloc_scratch(E, &e_atom);
     if (!msg.empty()) return msg;
     if (S == 0) return "";
     const int maxn = max_nodes(E);

@@ -378,13 +378,16 @@ int nnp_opt_reset(nnp_handle *h);
  *  device pointers on the handle's device, which must be current; n_atoms
  *  must equal d_atom_off[n_struct] (a structure whose offsets fall outside
  *  [0, n_atoms] gets a NaN energy).  flags: 0 or NNP_VACUUM.
+ * The networks are the FP32 ones: a handle set to NNP_PREC_BF16 or
+ * NNP_PREC_BF16X3 gets NNP_ERR_UNSUPPORTED (set NNP_PREC_FP32 first).
  * The kernels are queued on the handle's stream and the call returns without
  * waiting for them.  An atom type outside [0, ntypes) gives a NaN energy for
- * its structure.  The first call on a device looks up the scratch array's
- * address, which may load the library's device code; make that first call
- * before any stream capture.  The scratch array is one per device, shared by
- * all handles: calls that can overlap in time (other streams, other host
- * threads) race on it and must be ordered by the caller. */
+ * its structure.  The first call on a handle looks up the scratch array's
+ * device address (which may load the library's device code) and keeps it
+ * with the handle; make that first call before any stream capture.  The
+ * scratch array is one per device, shared by all handles: calls that can
+ * overlap in time (other streams, other host threads) race on it and must be
+ * ordered by the caller. */
 #define NNP_NOALLOC_MAX_ATOMS (1 << 20)
 int nnp_energy_symm_noalloc(nnp_handle *h, int32_t n_struct, int64_t n_atoms, const int64_t *d_atom_off,
                             const int32_t *d_type, const float *d_symm, int32_t gstride, uint32_t flags,
