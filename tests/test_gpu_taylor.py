@@ -100,14 +100,14 @@ def test_first_order_energies_against_model(tmp_path):
     nn = NNP.read(path)
     E, F = nn.compute_batch(b.atom_off, b.pos, b.type, b.cell)
     errs = {}
-    for w in (1e-3, 2e-3):
+    for w in (0.01, 0.02):       # wide enough that the second-order term dwarfs the FP32 energy noise (~3e-6 eV)
         oo, op, ot, oe, src = taylor_expand(b.atom_off, b.pos, b.type, E, F, 2, "UNIFORM", w, seed=7)
         Em, _ = nn.compute_batch(oo, op, ot, b.cell[src])
         errs[w] = np.abs(Em - oe).max()
     nn.close()
-    print("first-order error: %.3e (w 1e-3), %.3e (w 2e-3)" % (errs[1e-3], errs[2e-3]))
-    assert errs[1e-3] < 1e-3
-    assert 2.0 < errs[2e-3] / max(errs[1e-3], 1e-15) < 8.0       # second order: x4 for twice the width
+    print("first-order error: %.3e (w 0.01), %.3e (w 0.02)" % (errs[0.01], errs[0.02]))
+    assert errs[0.01] < 0.05
+    assert 2.5 < errs[0.02] / max(errs[0.01], 1e-15) < 6.0       # second order: x4 for twice the width
 
 
 def test_errors():
