@@ -71,7 +71,7 @@ void Engine::free_all()
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();
-    adam_idx.release(); adam_p.release(); adam_m.release(); adam_v.release();
+    adam_idx.release(); adam_p.release(); adam_m.release(); adam_v.release(); adam_wmask.release();
     graph_release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
@@ -1202,7 +1202,55 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
     return NNP_OK;
 }
 
+namespace {
+int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta);
+}
+
 int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
+{
+    return opt_adam_impl(h, gamma, eps, -1, 0.0);
+}
+
+int nnp_decay_step(int32_t kind, double alpha, int32_t period, double gamma, int32_t step, double *out)
+{
+    if (!out) return NNP_ERR_ARG;
+    switch (kind) {
+    case NNP_DECAY_CONST: *out = gamma; break;
+    case NNP_DECAY_EXP: *out = gamma * (1.0 - alpha); break;
+    case NNP_DECAY_GAUSS: *out = gamma * (1.0 - 2.0 * alpha * step); break;
+    case NNP_DECAY_SQRT: *out = gamma * (1.0 - 0.5 * alpha / (1.0 + alpha * step)); break;
+    case NNP_DECAY_INV: *out = gamma * (1.0 - alpha / (1.0 + alpha * step)); break;
+    case NNP_DECAY_STEP:
+        if (period <= 0) {
+            g_create_error = "opt::Decay: STEP needs a positive period";
+            return NNP_ERR_ARG;
+        }
+        *out = (step > 0 && (unsigned)step % (unsigned)period == 0) ? gamma * alpha : gamma;
+        break;
+    default:
+        g_create_error = "opt::Decay::step(const Objective&,const Iterator&): invalid decay method.";
+        return NNP_ERR_ARG;
+    }
+    return NNP_OK;
+}
+
+int nnp_opt_step(nnp_handle *h, double *gamma, int32_t step, int32_t decay_kind, double alpha, int32_t period,
+                 int32_t reg_kind, double eta, double eps)
+{
+    if (!h || !gamma) return NNP_ERR_ARG;
+    if (reg_kind < NNP_REG_LASSO || reg_kind > NNP_REG_NONE) return fail(h, NNP_ERR_ARG, "invalid regularization");
+    if (alpha < 0) return fail(h, NNP_ERR_ARG, "opt::Decay::read(Token&): invalid alpha.");
+    double g = 0.0;
+    if (nnp_decay_step(decay_kind, alpha, period, *gamma, step, &g) != NNP_OK) return fail(h, NNP_ERR_ARG, g_create_error);
+    const int rc = opt_adam_impl(h, g, eps, reg_kind == NNP_REG_NONE ? -1 : reg_kind, eta);
+    if (rc == NNP_OK) *gamma = g;
+    return rc;
+}
+
+}  // extern "C"
+
+namespace {
+int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta)
 {
     if (!h) return NNP_ERR_ARG;
     nnp::Engine &E = h->E;
@@ -1243,6 +1291,13 @@ int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
         const bool fresh = E.adam_idx_host.size() != idx.size();
         E.adam_idx_host = idx;
         const size_t n = idx.size();
+        std::vector<unsigned char> wm;
+        for (int t = 0; t < E.dpot.ntypes; ++t) {
+            const nnp::DevType &T = E.dpot.t[t];
+            for (int l = 0; l < T.nlayer; ++l) wm.insert(wm.end(), T.nodes[l + 1], 0);
+            for (int l = 0; l < T.nlayer; ++l) wm.insert(wm.end(), (size_t)T.nodes[l] * T.nodes[l + 1], 1);
+        }
+        chk(E.adam_wmask.reserve(n));
         chk(E.adam_idx.reserve(n));
         chk(E.adam_p.reserve(n));
         chk(E.adam_m.reserve(n));
@@ -1250,6 +1305,7 @@ int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
         if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
         chk(cudaMemcpyAsync(E.adam_idx.p, idx.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, E.stream));
         chk(cudaMemcpyAsync(E.adam_p.p, val.data(), sizeof(double) * n, cudaMemcpyHostToDevice, E.stream));
+        chk(cudaMemcpyAsync(E.adam_wmask.p, wm.data(), n, cudaMemcpyHostToDevice, E.stream));
         if (fresh) {        // first step (ADAM::resize): zero averages, powers beta^1
             chk(cudaMemsetAsync(E.adam_m.p, 0, sizeof(double) * n, E.stream));
             chk(cudaMemsetAsync(E.adam_v.p, 0, sizeof(double) * n, E.stream));
@@ -1260,7 +1316,7 @@ int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
         if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("ADAM set-up failed: ") + cudaGetErrorString(ce));
         E.adam_master_stale = false;
     }
-    std::string msg = nnp::run_adam(E, gamma, eps);
+    std::string msg = nnp::run_adam(E, gamma, eps, reg, eta);
     if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
     // mirror the new parameters into the host model (nnp_get_params, nnp_write)
     std::vector<double> val(E.adam_idx_host.size());
@@ -1282,6 +1338,9 @@ int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
     E.grad_valid = false;
     return NNP_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int nnp_opt_reset(nnp_handle *h)
 {

@@ -140,6 +140,7 @@ struct Engine {
     std::vector<int64_t> adam_idx_host;
     DBuf<int64_t> adam_idx;
     DBuf<double> adam_p, adam_m, adam_v;
+    DBuf<unsigned char> adam_wmask;   // 1 for a weight, 0 for a bias (the weight-decay mask)
     double adam_b1i = 0.9, adam_b2i = 0.999;
     bool adam_master_stale = true;  // the master copy must be reloaded from the host model
     int loss_kind = 1;            // energy-loss kind of nnp_train_grad (NNP_LOSS_*)
@@ -187,7 +188,7 @@ std::string run_atom_energy(Engine &E, bool vacuum, double *out);
 std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
 std::string run_train_grad(Engine &E, bool with_force);
-std::string run_adam(Engine &E, double gamma, double eps);
+std::string run_adam(Engine &E, double gamma, double eps, int reg, double eta);
 std::string run_input_stats(Engine &E, std::vector<int64_t> &count, std::vector<double> &stats);
 std::string taylor_expand(int S, const int64_t *atom_off, const double *pos, const double *energy,
                           const double *forces, int nadd, int dist, double rdelta, uint64_t seed,

@@ -229,9 +229,14 @@ namespace nnp {
 // the device (grad, wpar layout, at idx[i]): running averages m, v of the
 // gradient and its square, p -= gamma b1ii m / (sqrt(b2ii v) + eps) on the
 // FP64 master copy p64, and its FP32 value written into the networks' table.
+// After the step, nnptefr's weight decay (nnptefr.cpp:1034-1057) of kind reg
+// (0 LASSO sgn(p), 1 RIDGE p, 2 HUBER p / sqrt(1 + p^2), 3 ASINH asinh(p),
+// anything else none) with strength gamma * eta on the weights (wmask 1; the
+// biases have 0), evaluated at the parameters before the step.
 __global__ void k_adam(int64_t n, const int64_t *__restrict__ idx, const double *__restrict__ grad,
                        double *__restrict__ p64, double *__restrict__ m, double *__restrict__ v,
-                       float *__restrict__ wpar, double gamma, double b1ii, double b2ii, double eps)
+                       float *__restrict__ wpar, double gamma, double b1ii, double b2ii, double eps,
+                       const unsigned char *__restrict__ wmask, int reg, double eta)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -244,18 +249,27 @@ __global__ void k_adam(int64_t n, const int64_t *__restrict__ idx, const double 
     vv += (1.0 - beta2) * g * g;
     m[i] = mm;
     v[i] = vv;
-    const double p = p64[i] - gamma * b1ii * mm / (sqrt(b2ii * vv) + eps);
+    const double po = p64[i];
+    double p = po - gamma * b1ii * mm / (sqrt(b2ii * vv) + eps);
+    if (reg >= 0 && reg <= 3 && wmask[i]) {
+        const double f = reg == 0 ? (double)((po > 0) - (po < 0))
+                         : reg == 1 ? po
+                         : reg == 2 ? po / sqrt(1.0 + po * po)
+                                    : asinh(po);
+        p -= gamma * eta * f;
+    }
     p64[i] = p;
     wpar[idx[i]] = (float)p;
 }
 
-std::string run_adam(Engine &E, double gamma, double eps)
+std::string run_adam(Engine &E, double gamma, double eps, int reg, double eta)
 {
     const int64_t n = (int64_t)E.adam_idx_host.size();
     if (n == 0) return "";
     const double b1ii = 1.0 / (1.0 - E.adam_b1i), b2ii = 1.0 / (1.0 - E.adam_b2i);
     k_adam<<<(int)((n + 255) / 256), 256, 0, E.stream>>>(n, E.adam_idx.p, E.pgrad.p, E.adam_p.p, E.adam_m.p,
-                                                           E.adam_v.p, E.wpar.p, gamma, b1ii, b2ii, eps);
+                                                           E.adam_v.p, E.wpar.p, gamma, b1ii, b2ii, eps,
+                                                           E.adam_wmask.p, reg, eta);
     E.launches += 1;
     E.adam_b1i *= 0.9;
     E.adam_b2i *= 0.999;

@@ -24,6 +24,8 @@ ERRORS = {-1: "ARG", -2: "IO", -3: "PARSE", -4: "CUDA", -5: "CAPACITY", -6: "UNS
 PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
 ACC_FP32, ACC_FP64, SYMM_FP64 = 0, 1, 2
 LOSS_MSE, LOSS_MAE, LOSS_HUBER, LOSS_ASINH = 1, 2, 3, 4   # opt::Loss (opt/loss.hpp:18-24)
+DECAY = {"CONST": 1, "EXP": 2, "GAUSS": 3, "SQRT": 4, "INV": 5, "STEP": 6}   # opt::Decay::Name
+REG = {"LASSO": 0, "RIDGE": 1, "HUBER": 2, "ASINH": 3, "NONE": 4}              # Regularization
 STATS = ("max", "min", "harmonic", "mean", "dev", "rms")   # nnp_input_stats, NNP_STAT_* order
 PREBIAS = {"IDENTITY": 0, "MEAN": 1, "HAR": 2, "RMS": 3, "MID": 4, "MIN": 5}      # nnptefr.hpp:97-107
 PRESCALE = {"IDENTITY": 0, "DEV": 1, "MINMAX": 2, "MAX": 3}                     # nnptefr.hpp:69-77
@@ -80,6 +82,8 @@ def lib():
             "nnp_set_loss": ([p, i, d], i),
             "nnp_opt_adam": ([p, d, d], i),
             "nnp_opt_reset": ([p], i),
+            "nnp_opt_step": ([p, C.POINTER(d), i, i, d, i, i, d, d], i),
+            "nnp_decay_step": ([i, d, i, d, i, C.POINTER(d)], i),
             "nnp_set_mma_wait": ([p, C.c_int64], i),
             "nnp_set_autotune": ([p, i], i),
             "nnp_tune_params": ([p, p, i, C.POINTER(i), C.POINTER(C.c_char_p)], i),
@@ -198,6 +202,17 @@ class NNP:
     def opt_adam(self, gamma: float, eps: float = 1e-16):
         """One ADAM step on the device with the last train_grad gradient."""
         self._check(lib().nnp_opt_adam(self._h, float(gamma), float(eps)))
+
+    def opt_step(self, gamma: float, step: int, decay="CONST", alpha=0.0, period=0, reg="NONE", eta=0.0,
+                 eps: float = 1e-16) -> float:
+        """nnptefr's optimiser step on the device: decayed rate, ADAM, weight
+        decay; returns the rate used."""
+        g = C.c_double(gamma)
+        dk = DECAY[decay] if isinstance(decay, str) else decay
+        rk = REG[reg] if isinstance(reg, str) else reg
+        self._check(lib().nnp_opt_step(self._h, C.byref(g), int(step), int(dk), float(alpha), int(period), int(rk),
+                                       float(eta), float(eps)))
+        return g.value
 
     def opt_reset(self):
         self._check(lib().nnp_opt_reset(self._h))
@@ -521,3 +536,13 @@ def read_structures(path: str, type_names, fmt: str = "xyz"):
     if rc != NNP_OK:
         raise NNPError(rc, lib().nnp_last_error(None).decode())
     return off, pos[:N], typ[:N], cell[:S], pbc[:S].astype(bool), en[:S], frc[:N]
+
+
+def decay_step(kind, alpha, period, gamma, step):
+    """opt::Decay::step: the next learning rate (host only)."""
+    out = C.c_double()
+    rc = lib().nnp_decay_step(DECAY[kind] if isinstance(kind, str) else kind, float(alpha), int(period), float(gamma),
+                              int(step), C.byref(out))
+    if rc != NNP_OK:
+        raise NNPError(rc, lib().nnp_last_error(None).decode())
+    return out.value

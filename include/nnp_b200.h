@@ -365,6 +365,31 @@ int nnp_set_loss(nnp_handle *h, int32_t kind, double delta);
 int nnp_opt_adam(nnp_handle *h, double gamma, double eps);
 int nnp_opt_reset(nnp_handle *h);
 
+/* The learning-rate schedules of opt::Decay::step (opt/decay.cpp:58-82,
+ * names decay.hpp:28-36): the rate of the next step from the current one,
+ * at iteration step.  Host only; errors in nnp_last_error(NULL). */
+#define NNP_DECAY_CONST 1   /* gamma                                           */
+#define NNP_DECAY_EXP 2     /* gamma (1 - alpha)                               */
+#define NNP_DECAY_GAUSS 3   /* gamma (1 - 2 alpha step)                        */
+#define NNP_DECAY_SQRT 4    /* gamma (1 - alpha / 2 / (1 + alpha step))       */
+#define NNP_DECAY_INV 5     /* gamma (1 - alpha / (1 + alpha step))           */
+#define NNP_DECAY_STEP 6    /* gamma alpha when step > 0 is a multiple of period */
+int nnp_decay_step(int32_t kind, double alpha, int32_t period, double gamma, int32_t step, double *out);
+
+/* One optimiser step of nnptefr's loop (nnptefr.cpp:1032-1057) on the device:
+ * *gamma = decay(*gamma, step), the ADAM step of nnp_opt_adam with it, then
+ * weight decay of the weights (not the biases) at their values before the
+ * step, p -= gamma eta r(p): regularization (nnptefr.hpp:183-191) LASSO
+ * sgn(p), RIDGE p, HUBER p / sqrt(1 + p^2), ASINH asinh(p), or NONE.
+ * *gamma receives the rate used. */
+#define NNP_REG_LASSO 0
+#define NNP_REG_RIDGE 1
+#define NNP_REG_HUBER 2
+#define NNP_REG_ASINH 3
+#define NNP_REG_NONE 4
+int nnp_opt_step(nnp_handle *h, double *gamma, int32_t step, int32_t decay_kind, double alpha, int32_t period,
+                 int32_t reg_kind, double eta, double eps);
+
 /* Allocation-free energies from device-resident symmetry functions (no
  * counterpart in the reference, whose NNP::compute_energy (nnp.cpp:329-338)
  * it otherwise follows).  For callers that must not allocate device memory

@@ -37,6 +37,8 @@ def lib():
         L.ref_nnp_compute.argtypes = [p, C.c_int, dp, C.POINTER(C.c_int), dp, C.c_int, C.c_int, dp, dp, dp, dp,
                                       C.c_char_p, C.c_int]
         L.ref_nnp_nparams.argtypes = [p, C.c_int]
+        L.ref_decay_step.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int]
+        L.ref_decay_step.restype = C.c_double
         L.ref_read_structure.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp, dp, dp,
                                          C.c_char_p, C.c_int, C.c_char_p, C.c_int]
         L.ref_energy_loss_grad.argtypes = [p, C.c_int, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int), dp, C.c_int,

@@ -16,6 +16,8 @@
 #include "format/vasp_struc.hpp"
 #include "format/xyz_struc.hpp"
 #include "ml/nn.hpp"
+#include "opt/decay.hpp"
+#include "opt/iter.hpp"
 #include "nnp/nnp.hpp"
 #include "struc/neighbor.hpp"
 #include "struc/structure.hpp"
@@ -314,6 +316,17 @@ int ref_read_structure(const char *path, int format, int cap, int *n, double *po
         put(err, errlen, e.what());
     }
     return -1;
+}
+
+// opt::Decay::step (opt/decay.cpp:58-82) of decay kind `kind` (opt::Decay::Name)
+// with alpha and period at iteration step.
+double ref_decay_step(int kind, double alpha, int period, double gamma, int step)
+{
+    opt::Decay d(static_cast<opt::Decay::Name::Type>(kind), alpha);
+    d.period() = period;
+    opt::Iterator it;
+    it.step() = step;
+    return d.step(gamma, it);
 }
 
 }  // extern "C"

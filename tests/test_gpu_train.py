@@ -196,3 +196,35 @@ def test_device_training_loop_reduces_loss(tmp_path):
     nn.close()
     print("loss %.4e -> %.4e" % (losses[0], losses[-1]))
     assert losses[-1] < 0.5 * losses[0]
+
+
+@pytest.mark.parametrize("reg", ["NONE", "LASSO", "RIDGE", "HUBER", "ASINH"])
+def test_opt_step_matches_nnptefr_sequence(tmp_path, reg):
+    """nnp_opt_step = nnptefr's decay, ADAM step and weight decay of the
+    weights (nnptefr.cpp:1032-1057), three steps, against a restatement."""
+    from ace_b200.nnp import decay_step
+    b, path, e_ref, f_ref = setup(tmp_path, n=3, seed=81)
+    nn = NNP.read(path)
+    p = nn.get_params()
+    counts = [nn.nparams(t) for t in range(nn.ntypes)]
+    # weight mask: per type, biases then weights (nnptefr.cpp:916-929)
+    pot = potential.read(path)
+    wm = np.concatenate([np.concatenate([np.zeros(sum(net.nodes[1:])),
+                                         np.ones(sum(a * c for a, c in zip(net.nodes[:-1], net.nodes[1:])))])
+                         for net in pot.nets])
+    assert len(wm) == sum(counts)
+    rfun = {"NONE": lambda x: 0 * x, "LASSO": np.sign, "RIDGE": lambda x: x,
+            "HUBER": lambda x: x / np.sqrt(1 + x * x), "ASINH": np.arcsinh}[reg]
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    g_rate = g_ref = 2e-3
+    for t in range(1, 4):
+        _, g, _, _ = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, 0.5, norm_mode=1)
+        g_rate = nn.opt_step(g_rate, t, "INV", 0.1, 0, reg, 1e-2)
+        g_ref = decay_step("INV", 0.1, 0, g_ref, t)
+        assert g_rate == g_ref
+        pold = p.copy()
+        p, m, v = adam_reference(p, g, m, v, t, g_ref)
+        p = p - g_ref * 1e-2 * wm * rfun(pold)
+        assert np.abs(nn.get_params() - p).max() <= 1e-12 * np.abs(p).max()
+    nn.close()
