@@ -72,6 +72,7 @@ void Engine::free_all()
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();
     adam_idx.release(); adam_p.release(); adam_m.release(); adam_v.release(); adam_wmask.release();
+    loss_part.release(); train_ref.release(); grad_pack.release(); pack_idx.release();
     graph_release();
     jit_release(*this);
     if (d_pot) cudaFree(d_pot);
@@ -666,6 +667,10 @@ namespace {
 
 // nnp_compute and nnp_compute_md: the whole pipeline, with the optional
 // per-atom energies [N] and per-structure virials [9 S] of the MD call.
+// internal flag of compute_impl: energies and forces are computed into the
+// handle's buffers (e_struct, force) and the output pointers may be NULL
+constexpr uint32_t KEEP_ON_DEVICE = 1u << 30;
+
 int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forces, double *symm_out,
                  double *atom_energy, double *virial, uint32_t flags, int64_t n_ghost = 0)
 {
@@ -673,8 +678,8 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
     nnp::Engine &E = h->E;
     E.n_ghost = n_ghost;
     if (b->n_struct < 0) return fail(h, NNP_ERR_ARG, "negative structure count");
-    if ((flags & NNP_ENERGY) && !energy) return fail(h, NNP_ERR_ARG, "energy output missing");
-    if ((flags & NNP_FORCES) && !forces) return fail(h, NNP_ERR_ARG, "force output missing");
+    if ((flags & NNP_ENERGY) && !energy && !(flags & KEEP_ON_DEVICE)) return fail(h, NNP_ERR_ARG, "energy output missing");
+    if ((flags & NNP_FORCES) && !forces && !(flags & KEEP_ON_DEVICE)) return fail(h, NNP_ERR_ARG, "force output missing");
     if ((flags & NNP_SYMM) && !symm_out) return fail(h, NNP_ERR_ARG, "symmetry-function output missing");
     const int S = b->n_struct;
     if (S == 0) return NNP_OK;
@@ -843,8 +848,8 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
         // outputs
         if (!devp) {
             const size_t be = sizeof(double) * S, bf = sizeof(double) * 3 * N;
-            if (flags & NNP_ENERGY) chk(cudaMemcpyAsync(energy, E.e_struct.p, be, cudaMemcpyDeviceToHost, E.stream));
-            if (flags & NNP_FORCES) chk(cudaMemcpyAsync(forces, E.force.p, bf, cudaMemcpyDeviceToHost, E.stream));
+            if ((flags & NNP_ENERGY) && energy) chk(cudaMemcpyAsync(energy, E.e_struct.p, be, cudaMemcpyDeviceToHost, E.stream));
+            if ((flags & NNP_FORCES) && forces) chk(cudaMemcpyAsync(forces, E.force.p, bf, cudaMemcpyDeviceToHost, E.stream));
             if (flags & NNP_SYMM) {
                 chk(E.symm_d.reserve((size_t)N * E.gstride + 1));
                 nnp::run_symm_to_double(E, E.symm_d.p);
@@ -857,8 +862,8 @@ int compute_impl(nnp_handle *h, const nnp_batch *b, double *energy, double *forc
             }
             if (virial) chk(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost, E.stream));
         } else {
-            if (flags & NNP_ENERGY) chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToDevice, E.stream));
-            if (flags & NNP_FORCES) chk(cudaMemcpyAsync(forces, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, E.stream));
+            if ((flags & NNP_ENERGY) && energy) chk(cudaMemcpyAsync(energy, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToDevice, E.stream));
+            if ((flags & NNP_FORCES) && forces) chk(cudaMemcpyAsync(forces, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, E.stream));
             if (flags & NNP_SYMM) nnp::run_symm_to_double(E, symm_out);
             if (atom_energy) nnp::run_atom_energy(E, (flags & NNP_VACUUM) != 0, atom_energy);
             if (virial) chk(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9 * S, cudaMemcpyDeviceToDevice, E.stream));
@@ -1204,7 +1209,40 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
 
 namespace {
 int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta);
+
+// wpar offset of every network parameter in the reference packing (per type
+// in index order: biases by layer, then the weights column-major,
+// nn.cpp:881-915), and whether it is a weight
+void pack_offsets(const nnp::Engine &E, std::vector<int64_t> &idx, std::vector<unsigned char> *is_weight)
+{
+    idx.clear();
+    if (is_weight) is_weight->clear();
+    for (int t = 0; t < E.dpot.ntypes; ++t) {
+        const nnp::DevType &T = E.dpot.t[t];
+        const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+        int64_t off = T.woff + 2 * nin + 2 * nout;
+        std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
+        for (int l = 0; l < T.nlayer; ++l) {
+            boff[l] = off;
+            woff[l] = off + T.nodes[l + 1];
+            off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
+        }
+        for (int l = 0; l < T.nlayer; ++l)
+            for (int n = 0; n < T.nodes[l + 1]; ++n) {
+                idx.push_back(boff[l] + n);
+                if (is_weight) is_weight->push_back(0);
+            }
+        for (int l = 0; l < T.nlayer; ++l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) {
+                    idx.push_back(woff[l] + (int64_t)m * st + n);
+                    if (is_weight) is_weight->push_back(1);
+                }
+        }
+    }
 }
+}  // namespace
 
 int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
 {
@@ -1260,43 +1298,23 @@ int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta)
     cudaError_t ce = cudaSuccess;
     auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
     if (E.adam_master_stale) {
-        // parameters in the reference packing: their wpar offsets and FP64 values
+        // parameters in the reference packing: their wpar offsets, weight mask and FP64 values
         std::vector<int64_t> idx;
+        std::vector<unsigned char> wm;
+        pack_offsets(E, idx, &wm);
         std::vector<double> val;
-        for (int t = 0; t < E.dpot.ntypes; ++t) {
-            const nnp::DevType &T = E.dpot.t[t];
-            const nnp::HostNet &net = E.host.nets[t];
-            const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
-            int64_t off = T.woff + 2 * nin + 2 * nout;
-            std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
-            for (int l = 0; l < T.nlayer; ++l) {
-                boff[l] = off;
-                woff[l] = off + T.nodes[l + 1];
-                off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
-            }
-            for (int l = 0; l < T.nlayer; ++l)
-                for (int n = 0; n < T.nodes[l + 1]; ++n) {
-                    idx.push_back(boff[l] + n);
-                    val.push_back(net.b[l][n]);
-                }
-            for (int l = 0; l < T.nlayer; ++l) {
-                const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
+        for (const auto &net : E.host.nets) {
+            const int nl = (int)net.nodes.size() - 1;
+            for (int l = 0; l < nl; ++l) val.insert(val.end(), net.b[l].begin(), net.b[l].end());
+            for (int l = 0; l < nl; ++l) {
+                const int ni = net.nodes[l], no = net.nodes[l + 1];
                 for (int m = 0; m < ni; ++m)
-                    for (int n = 0; n < no; ++n) {
-                        idx.push_back(woff[l] + (int64_t)m * st + n);
-                        val.push_back(net.w[l][(size_t)n * ni + m]);
-                    }
+                    for (int n = 0; n < no; ++n) val.push_back(net.w[l][(size_t)n * ni + m]);
             }
         }
         const bool fresh = E.adam_idx_host.size() != idx.size();
         E.adam_idx_host = idx;
         const size_t n = idx.size();
-        std::vector<unsigned char> wm;
-        for (int t = 0; t < E.dpot.ntypes; ++t) {
-            const nnp::DevType &T = E.dpot.t[t];
-            for (int l = 0; l < T.nlayer; ++l) wm.insert(wm.end(), T.nodes[l + 1], 0);
-            for (int l = 0; l < T.nlayer; ++l) wm.insert(wm.end(), (size_t)T.nodes[l] * T.nodes[l + 1], 1);
-        }
         chk(E.adam_wmask.reserve(n));
         chk(E.adam_idx.reserve(n));
         chk(E.adam_p.reserve(n));
@@ -1431,8 +1449,10 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, c
 {
     if (!h || !batch) return NNP_ERR_ARG;
     nnp::Engine &E = h->E;
-    if (flags & NNP_DEVICE_PTRS) return fail(h, NNP_ERR_UNSUPPORTED, "nnp_train_grad takes host pointers");
-    if (!e_ref || !loss || !grad) return fail(h, NNP_ERR_ARG, "e_ref, loss and grad are required");
+    if (flags & ~(uint32_t)NNP_DEVICE_PTRS) return fail(h, NNP_ERR_ARG, "flags other than NNP_DEVICE_PTRS");
+    const bool devp = (flags & NNP_DEVICE_PTRS) != 0;
+    if (!e_ref || !loss) return fail(h, NNP_ERR_ARG, "e_ref and loss are required");
+    if (!grad && !devp) return fail(h, NNP_ERR_ARG, "grad is required with host pointers");
     if (w_f != 0.0 && !f_ref) return fail(h, NNP_ERR_ARG, "f_ref is required when w_f is nonzero");
     if (!(w_f >= 0.0)) return fail(h, NNP_ERR_ARG, "w_f must be non-negative");
     if (norm_mode < 0 || norm_mode > 4) return fail(h, NNP_ERR_ARG, "unknown norm mode");
@@ -1442,112 +1462,75 @@ int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref, c
         for (const auto &net : E.host.nets)
             if (net.neuron != nnp::NEU_LINEAR && net.neuron != nnp::NEU_SIGMOID && net.neuron != nnp::NEU_TANH)
                 return fail(h, NNP_ERR_UNSUPPORTED, "the force term needs f'' of the activation (LINEAR, SIGMOID or TANH)");
-    // forward: energies (no vacuum terms, as nnptefr subtracts them from the labels) and forces
-    const int64_t N = batch->atom_off[S];
-    std::vector<double> Eh(S), Fh((size_t)std::max<int64_t>(N, 1) * 3);
-    // the gradient kernels run the FP32 networks, so the forward pass does too
+    E.grad_valid = false;
+    // forward: energies (no vacuum terms, as nnptefr subtracts them from the
+    // labels) and forces, kept in the handle's buffers; the gradient kernels
+    // run the FP32 networks, so the forward pass does too
     const int prec = E.precision;
     E.precision = NNP_PREC_FP32;
-    int rc = nnp_compute(h, batch, Eh.data(), Fh.data(), nullptr, NNP_ENERGY | NNP_FORCES);
+    int rc = compute_impl(h, batch, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          NNP_ENERGY | NNP_FORCES | KEEP_ON_DEVICE | (devp ? NNP_DEVICE_PTRS : 0u));
     E.precision = prec;
     if (rc != NNP_OK) return rc;
-    // loss and the per-structure / per-atom factors (nnptefr.cpp:614-620 norms)
-    std::vector<float> ge((size_t)std::max<int64_t>(N, 1));
-    std::vector<float4> tv((size_t)std::max<int64_t>(N, 1), make_float4(0.f, 0.f, 0.f, 0.f));
-    const double bi = 1.0 / S;
-    double L = 0.0;
-    for (int s = 0; s < S; ++s) {
-        const int64_t a0 = batch->atom_off[s], a1 = batch->atom_off[s + 1];
-        const double nat = (double)(a1 - a0);
-        double nrm = 1.0;
-        switch (norm_mode) {
-        case 1: nrm = 1.0 / nat; break;
-        case 2: nrm = 1.0 / std::sqrt(nat); break;
-        case 3: nrm = 1.0 / std::cbrt(nat); break;
-        case 4: nrm = 1.0 / (std::log(nat) + 1.0); break;
-        default: break;
-        }
-        // energy term: NNPTEFR::error_cost_o1's loss and gradient factor (nnptefr.cpp:1340-1376)
-        const double dU = (Eh[s] - e_ref[s]) * nrm;
-        double gf = nrm * bi;
-        switch (E.loss_kind) {
-        case NNP_LOSS_MAE:
-            L += bi * std::fabs(dU);
-            gf *= (dU > 0) - (dU < 0);
-            break;
-        case NNP_LOSS_HUBER: {
-            const double arg = dU / E.loss_delta, sq = std::sqrt(1.0 + arg * arg);
-            L += bi * E.loss_delta * E.loss_delta * (sq - 1.0);
-            gf *= dU / sq;
-        } break;
-        case NNP_LOSS_ASINH: {
-            const double arg = dU / E.loss_delta, sq = std::sqrt(1.0 + arg * arg), lg = std::log(arg + sq);
-            L += bi * E.loss_delta * E.loss_delta * (1.0 - sq + arg * lg);
-            gf *= lg * E.loss_delta;
-        } break;
-        default:
-            L += bi * 0.5 * dU * dU;
-            gf *= dU;
-            break;
-        }
-        const double fs = nat > 0 ? w_f / (3.0 * nat) : 0.0;
-        double lf = 0.0;
-        for (int64_t a = a0; a < a1; ++a) {
-            ge[a] = (float)gf;
-            if (w_f != 0.0) {
-                double d[3];
-                for (int k = 0; k < 3; ++k) {
-                    d[k] = Fh[3 * a + k] - f_ref[3 * a + k];
-                    lf += d[k] * d[k];
-                }
-                tv[a] = make_float4((float)(fs * d[0] * bi), (float)(fs * d[1] * bi), (float)(fs * d[2] * bi), 0.f);
-            }
-        }
-        L += bi * 0.5 * fs * lf;
-    }
+    const int64_t N = E.n_atoms;
     cudaError_t ce = cudaSuccess;
     auto chk = [&](cudaError_t x) { if (x != cudaSuccess && ce == cudaSuccess) ce = x; };
     chk(E.gE.reserve(std::max<int64_t>(N, 1)));
     chk(E.pgrad.reserve(E.wfloats));
-    if (w_f != 0.0) {
-        chk(E.tvec.reserve(std::max<int64_t>(N, 1)));
-        chk(E.tang.reserve((size_t)std::max<int64_t>(N, 1) * E.gstride));
+    chk(E.loss_part.reserve(S + 1));
+    chk(E.tvec.reserve(std::max<int64_t>(N, 1)));
+    if (w_f != 0.0) chk(E.tang.reserve((size_t)std::max<int64_t>(N, 1) * E.gstride));
+    if (!devp) chk(E.train_ref.reserve(S + 3 * (size_t)std::max<int64_t>(N, 1)));
+    if (E.pack_n == 0) {
+        std::vector<int64_t> idx;
+        pack_offsets(E, idx, nullptr);
+        chk(E.pack_idx.reserve(idx.size()));
+        chk(E.grad_pack.reserve(idx.size()));
+        if (ce == cudaSuccess)
+            chk(cudaMemcpyAsync(E.pack_idx.p, idx.data(), sizeof(int64_t) * idx.size(), cudaMemcpyHostToDevice, E.stream));
+        E.pack_n = (int64_t)idx.size();
     }
     if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("device allocation failed: ") + cudaGetErrorString(ce));
-    chk(cudaMemcpyAsync(E.gE.p, ge.data(), sizeof(float) * N, cudaMemcpyHostToDevice, E.stream));
-    if (w_f != 0.0) chk(cudaMemcpyAsync(E.tvec.p, tv.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+    // labels on the device
+    const double *er = e_ref, *fr = f_ref;
+    if (!devp) {
+        chk(cudaMemcpyAsync(E.train_ref.p, e_ref, sizeof(double) * S, cudaMemcpyHostToDevice, E.stream));
+        if (w_f != 0.0)
+            chk(cudaMemcpyAsync(E.train_ref.p + S, f_ref, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, E.stream));
+        er = E.train_ref.p;
+        fr = E.train_ref.p + S;
+    }
     if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("copy failed: ") + cudaGetErrorString(ce));
-    E.grad_valid = false;
-    std::string msg = nnp::run_train_grad(E, w_f != 0.0);
+    // loss and the per-atom factors on the device (nnptefr.cpp:1331-1380)
+    const int64_t *off = devp ? batch->atom_off : E.atom_off.p;
+    std::string msg = nnp::run_train_loss(E, off, er, fr, w_f, norm_mode, E.loss_part.p + S);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    // gradient kernels; with device pointers the batch's types are the caller's array
+    int *own_type = E.type.p;
+    if (devp) E.type.p = const_cast<int32_t *>(batch->type);
+    msg = nnp::run_train_grad(E, w_f != 0.0);
+    E.type.p = own_type;
     if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
     E.grad_valid = true;
-    std::vector<double> gw((size_t)E.wfloats);
-    chk(cudaMemcpyAsync(gw.data(), E.pgrad.p, sizeof(double) * E.wfloats, cudaMemcpyDeviceToHost, E.stream));
+    if (devp) {
+        chk(cudaMemcpyAsync(loss, E.loss_part.p + S, sizeof(double), cudaMemcpyDeviceToDevice, E.stream));
+        if (grad) {
+            msg = nnp::run_gather_grad(E, E.pack_idx.p, E.pack_n, grad);
+            if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+        }
+        if (e_out) chk(cudaMemcpyAsync(e_out, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToDevice, E.stream));
+        if (f_out) chk(cudaMemcpyAsync(f_out, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, E.stream));
+        if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("output copy failed: ") + cudaGetErrorString(ce));
+        return NNP_OK;
+    }
+    msg = nnp::run_gather_grad(E, E.pack_idx.p, E.pack_n, E.grad_pack.p);
+    if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
+    chk(cudaMemcpyAsync(loss, E.loss_part.p + S, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    chk(cudaMemcpyAsync(grad, E.grad_pack.p, sizeof(double) * E.pack_n, cudaMemcpyDeviceToHost, E.stream));
+    if (e_out) chk(cudaMemcpyAsync(e_out, E.e_struct.p, sizeof(double) * S, cudaMemcpyDeviceToHost, E.stream));
+    if (f_out) chk(cudaMemcpyAsync(f_out, E.force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, E.stream));
     chk(cudaStreamSynchronize(E.stream));
     if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("gradient failed: ") + cudaGetErrorString(ce));
-    // wpar layout -> reference packing (biases by layer, then column-major weights)
-    size_t k = 0;
-    for (int t = 0; t < E.dpot.ntypes; ++t) {
-        const nnp::DevType &T = E.dpot.t[t];
-        const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
-        int64_t off = T.woff + 2 * nin + 2 * nout;
-        std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
-        for (int l = 0; l < T.nlayer; ++l) {
-            boff[l] = off;
-            woff[l] = off + T.nodes[l + 1];
-            off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
-        }
-        for (int l = 0; l < T.nlayer; ++l)
-            for (int n = 0; n < T.nodes[l + 1]; ++n) grad[k++] = gw[boff[l] + n];
-        for (int l = 0; l < T.nlayer; ++l) {
-            const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
-            for (int m = 0; m < ni; ++m)
-                for (int n = 0; n < no; ++n) grad[k++] = gw[woff[l] + (int64_t)m * st + n];
-        }
-    }
-    *loss = L;
-    if (e_out) std::copy(Eh.begin(), Eh.end(), e_out);
-    if (f_out) std::copy(Fh.begin(), Fh.begin() + 3 * N, f_out);
     return NNP_OK;
 }
 

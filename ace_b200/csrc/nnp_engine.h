@@ -135,6 +135,11 @@ struct Engine {
     DBuf<float> tang;             // tangent symmetry functions C [N * gstride]
     DBuf<double> pgrad;           // parameter gradient in the wpar layout [wfloats]
     bool grad_valid = false;      // pgrad holds the gradient of the last nnp_train_grad
+    DBuf<double> loss_part;       // per-structure loss terms [S + 1] (the last entry: the batch loss)
+    DBuf<double> train_ref;       // device copies of host labels: e_ref [S], f_ref [3N]
+    DBuf<double> grad_pack;       // gradient in the reference packing (host-pointer calls)
+    DBuf<int64_t> pack_idx;       // wpar offset of every parameter in the reference packing
+    int64_t pack_n = 0;
     // ADAM state (nnp_opt_adam): wpar offsets of the parameters in the
     // reference packing, FP64 master copy and running averages
     std::vector<int64_t> adam_idx_host;
@@ -189,6 +194,9 @@ std::string run_nn_from_symm(Engine &E, const double *symm_d, int gstride_in);
 std::string run_neighbor_counts(Engine &E, int *d_counts);
 std::string run_train_grad(Engine &E, bool with_force);
 std::string run_adam(Engine &E, double gamma, double eps, int reg, double eta);
+std::string run_train_loss(Engine &E, const int64_t *off, const double *e_ref, const double *f_ref, double w_f,
+                           int norm_mode, double *loss_dev);
+std::string run_gather_grad(Engine &E, const int64_t *idx, int64_t n, double *out);
 std::string run_input_stats(Engine &E, std::vector<int64_t> &count, std::vector<double> &stats);
 std::string taylor_expand(int S, const int64_t *atom_off, const double *pos, const double *energy,
                           const double *forces, int nadd, int dist, double rdelta, uint64_t seed,

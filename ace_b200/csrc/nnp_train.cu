@@ -277,3 +277,115 @@ std::string run_adam(Engine &E, double gamma, double eps, int reg, double eta)
 }
 
 }  // namespace nnp
+
+namespace nnp {
+
+namespace {
+
+// nnptefr's normalisation of a structure's energy error (nnptefr.cpp:614-620)
+__device__ inline double norm_factor(int mode, double nat)
+{
+    switch (mode) {
+    case 1: return 1.0 / nat;
+    case 2: return 1.0 / sqrt(nat);
+    case 3: return 1.0 / cbrt(nat);
+    case 4: return 1.0 / (log(nat) + 1.0);
+    default: return 1.0;
+    }
+}
+
+// One block per structure: the energy term of NNPTEFR::error_cost_o1
+// (nnptefr.cpp:1331-1380: dU = norm (E - E_ref), the loss of kind loss_kind
+// and its factor gf = norm dloss/ddU) and the force term
+// 0.5 w_f / (3 N) sum |F - F_ref|^2; writes every atom's energy factor
+// gE = gf / B and force adjoint V = w_f (F - F_ref) / (3 N B), and the
+// structure's loss / B into part[s].
+__global__ void k_train_loss(const int64_t *__restrict__ off, const double *__restrict__ E,
+                             const double *__restrict__ e_ref, const double *__restrict__ F,
+                             const double *__restrict__ f_ref, double w_f, int norm_mode, int loss_kind, double delta,
+                             double bi, float *__restrict__ ge, float4 *__restrict__ tv, double *__restrict__ part)
+{
+    __shared__ double red[256];
+    const int s = blockIdx.x;
+    const int64_t a0 = off[s], a1 = off[s + 1];
+    const double nat = (double)(a1 - a0);
+    const double nrm = norm_factor(norm_mode, nat);
+    const double dU = (E[s] - e_ref[s]) * nrm;
+    double le, dl;
+    switch (loss_kind) {
+    case 2: le = fabs(dU); dl = (dU > 0) - (dU < 0); break;
+    case 3: { const double a = dU / delta, sq = sqrt(1.0 + a * a); le = delta * delta * (sq - 1.0); dl = dU / sq; } break;
+    case 4: {
+        const double a = dU / delta, sq = sqrt(1.0 + a * a), lg = log(a + sq);
+        le = delta * delta * (1.0 - sq + a * lg);
+        dl = lg * delta;
+    } break;
+    default: le = 0.5 * dU * dU; dl = dU; break;
+    }
+    const float gf = (float)(nrm * dl * bi);
+    const double fs = nat > 0 ? w_f / (3.0 * nat) : 0.0;
+    double lf = 0.0;
+    for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        ge[a] = gf;
+        if (w_f != 0.0) {
+            const double d0 = F[3 * a] - f_ref[3 * a], d1 = F[3 * a + 1] - f_ref[3 * a + 1],
+                         d2 = F[3 * a + 2] - f_ref[3 * a + 2];
+            lf += d0 * d0 + d1 * d1 + d2 * d2;
+            tv[a] = make_float4((float)(fs * d0 * bi), (float)(fs * d1 * bi), (float)(fs * d2 * bi), 0.f);
+        }
+    }
+    red[threadIdx.x] = lf;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[s] = bi * (le + 0.5 * fs * red[0]);
+}
+
+// sum of part[0..S) in a fixed order (one block)
+__global__ void k_sum_fixed(int S, const double *__restrict__ part, double *__restrict__ out)
+{
+    __shared__ double red[256];
+    double v = 0.0;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) v += part[s];
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// gradient from the networks' table layout into the reference packing
+__global__ void k_gather_grad(int64_t n, const int64_t *__restrict__ idx, const double *__restrict__ g,
+                              double *__restrict__ out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = g[idx[i]];
+}
+
+}  // namespace
+
+std::string run_train_loss(Engine &E, const int64_t *off, const double *e_ref, const double *f_ref, double w_f,
+                           int norm_mode, double *loss_dev)
+{
+    const int S = E.n_struct;
+    const double bi = 1.0 / S;
+    k_train_loss<<<S, 256, 0, E.stream>>>(off, E.e_struct.p, e_ref, E.force.p, f_ref, w_f, norm_mode, E.loss_kind,
+                                          E.loss_delta, bi, E.gE.p, E.tvec.p, E.loss_part.p);
+    k_sum_fixed<<<1, 256, 0, E.stream>>>(S, E.loss_part.p, loss_dev);
+    E.launches += 2;
+    return cuda_msg("training loss");
+}
+
+std::string run_gather_grad(Engine &E, const int64_t *idx, int64_t n, double *out)
+{
+    if (n == 0) return "";
+    k_gather_grad<<<(int)((n + 255) / 256), 256, 0, E.stream>>>(n, idx, E.pgrad.p, out);
+    E.launches += 1;
+    return cuda_msg("gradient gather");
+}
+
+}  // namespace nnp

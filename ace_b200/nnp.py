@@ -437,6 +437,16 @@ class NNP:
 
     compute = compute_force   # NNP::compute (nnp.cpp:489-494) = build + symm + force
 
+    def train_grad_device(self, atom_off_ptr: int, pos_ptr: int, type_ptr: int, cell_ptr: int, n_struct: int,
+                          e_ref_ptr: int, f_ref_ptr: int, w_f: float, loss_ptr: int, grad_ptr: int = 0,
+                          norm_mode: int = 1, pbc: bool = True):
+        """train_grad on device-resident arrays (raw CUDA pointers); loss and
+        grad (optional) are device pointers too."""
+        b = _Batch(n_struct, atom_off_ptr, pos_ptr, type_ptr, cell_ptr, 1 if pbc else 0)
+        self._check(lib().nnp_train_grad(self._h, C.byref(b), C.c_void_p(e_ref_ptr), C.c_void_p(f_ref_ptr or None),
+                                         float(w_f), norm_mode, C.c_void_p(loss_ptr), C.c_void_p(grad_ptr or None),
+                                         None, None, DEVICE_PTRS))
+
     def train_grad(self, atom_off, pos, types, cells, e_ref, f_ref, w_f, norm_mode=1, pbc=True):
         """Energy+force loss, its weight gradient, and the model's E and F."""
         atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)

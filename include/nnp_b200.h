@@ -248,7 +248,14 @@ int nnp_set_params(nnp_handle *h, const double *params);
  * E_s excludes vacuum energies (nnptefr subtracts them from the labels,
  * nnptefr.cpp:2958).  norm_mode: 0 IDENTITY, 1 LINEAR (1/N_s), 2 SQRT, 3 CBRT,
  * 4 LOG (nnptefr.cpp:614-620).  grad has nnp_nparams total entries in the
- * nnp_get_params order.  e_out / f_out (optional) receive the model's E, F. */
+ * nnp_get_params order.  e_out / f_out (optional) receive the model's E, F.
+ * The loss, its per-atom factors and the gradient are computed on the
+ * device, and the gradient stays on the handle for nnp_opt_adam /
+ * nnp_opt_step.  flags: 0 (host pointers) or NNP_DEVICE_PTRS: the batch
+ * arrays, e_ref, f_ref, loss (one double), grad, e_out and f_out are then
+ * device memory, grad may be NULL, and the call returns after one
+ * synchronisation (the forward pass's error check) with the rest queued on
+ * the handle's stream. */
 int nnp_train_grad(nnp_handle *h, const nnp_batch *batch, const double *e_ref,
                    const double *f_ref, double w_f, int32_t norm_mode, double *loss,
                    double *grad, double *e_out, double *f_out, uint32_t flags);

@@ -228,3 +228,36 @@ def test_opt_step_matches_nnptefr_sequence(tmp_path, reg):
         p = p - g_ref * 1e-2 * wm * rfun(pold)
         assert np.abs(nn.get_params() - p).max() <= 1e-12 * np.abs(p).max()
     nn.close()
+
+
+def test_device_pointer_training_matches_host(tmp_path):
+    """nnp_train_grad with every array on the device gives the host-pointer
+    call's loss and gradient (the same device arithmetic), and a device
+    loop of train_grad + opt_step lowers the loss without host copies."""
+    import torch
+    b, path, e_ref, f_ref = setup(tmp_path, n=5, seed=91)
+    nn = NNP.read(path)
+    L, g, eo, fo = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, 0.5, norm_mode=2)
+    dev = torch.device("cuda", 0)
+    off = torch.tensor(b.atom_off, device=dev)
+    pos = torch.tensor(b.pos, device=dev)
+    typ = torch.tensor(b.type, device=dev)
+    cell = torch.tensor(b.cell.reshape(-1, 9), device=dev)
+    er = torch.tensor(e_ref, device=dev)
+    fr = torch.tensor(f_ref, device=dev)
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+    grad = torch.zeros(len(g), dtype=torch.float64, device=dev)
+    nn.train_grad_device(off.data_ptr(), pos.data_ptr(), typ.data_ptr(), cell.data_ptr(), b.n_struct, er.data_ptr(),
+                         fr.data_ptr(), 0.5, loss.data_ptr(), grad.data_ptr(), norm_mode=2)
+    torch.cuda.synchronize()
+    assert abs(loss.item() - L) <= 1e-12 * abs(L)
+    assert np.abs(grad.cpu().numpy() - g).max() <= 1e-9 * np.abs(g).max()
+    losses = []
+    gamma = 2e-3
+    for t in range(1, 16):
+        nn.train_grad_device(off.data_ptr(), pos.data_ptr(), typ.data_ptr(), cell.data_ptr(), b.n_struct,
+                             er.data_ptr(), fr.data_ptr(), 0.5, loss.data_ptr(), 0, norm_mode=2)
+        losses.append(loss.item())
+        gamma = nn.opt_step(gamma, t, "EXP", 1e-3, 0, "NONE", 0.0)
+    nn.close()
+    assert losses[-1] < 0.7 * losses[0]
