@@ -55,6 +55,65 @@ bool is_pinned_or_device(const void *p, bool *device)
     return a.type == cudaMemoryTypeHost || *device;
 }
 
+int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta);
+
+// After device optimiser steps the parameters live in the device's FP64
+// master copy; copy them into the host model before it is read or re-uploaded.
+std::string host_params(nnp::Engine &E)
+{
+    if (!E.host_stale) return "";
+    std::vector<double> val(E.adam_idx_host.size());
+    cudaError_t ce = cudaMemcpyAsync(val.data(), E.adam_p.p, sizeof(double) * val.size(), cudaMemcpyDeviceToHost, E.stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E.stream);
+    if (ce != cudaSuccess) return std::string("parameter copy failed: ") + cudaGetErrorString(ce);
+    size_t k = 0;
+    for (auto &net : E.host.nets) {
+        const int nl = (int)net.nodes.size() - 1;
+        for (int l = 0; l < nl; ++l)
+            for (auto &v : net.b[l]) v = val[k++];
+        for (int l = 0; l < nl; ++l) {
+            const int ni = net.nodes[l], no = net.nodes[l + 1];
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) net.w[l][(size_t)n * ni + m] = val[k++];
+        }
+    }
+    for (size_t i = 0; i < E.adam_idx_host.size(); ++i) E.wpar_host[E.adam_idx_host[i]] = (float)val[i];
+    E.host_stale = false;
+    return "";
+}
+
+// wpar offset of every network parameter in the reference packing (per type
+// in index order: biases by layer, then the weights column-major,
+// nn.cpp:881-915), and whether it is a weight
+void pack_offsets(const nnp::Engine &E, std::vector<int64_t> &idx, std::vector<unsigned char> *is_weight)
+{
+    idx.clear();
+    if (is_weight) is_weight->clear();
+    for (int t = 0; t < E.dpot.ntypes; ++t) {
+        const nnp::DevType &T = E.dpot.t[t];
+        const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
+        int64_t off = T.woff + 2 * nin + 2 * nout;
+        std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
+        for (int l = 0; l < T.nlayer; ++l) {
+            boff[l] = off;
+            woff[l] = off + T.nodes[l + 1];
+            off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
+        }
+        for (int l = 0; l < T.nlayer; ++l)
+            for (int n = 0; n < T.nodes[l + 1]; ++n) {
+                idx.push_back(boff[l] + n);
+                if (is_weight) is_weight->push_back(0);
+            }
+        for (int l = 0; l < T.nlayer; ++l) {
+            const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
+            for (int m = 0; m < ni; ++m)
+                for (int n = 0; n < no; ++n) {
+                    idx.push_back(woff[l] + (int64_t)m * st + n);
+                    if (is_weight) is_weight->push_back(1);
+                }
+        }
+    }
+}
 }  // namespace
 
 namespace nnp {
@@ -474,6 +533,8 @@ int nnp_destroy(nnp_handle *h)
 int nnp_write(const nnp_handle *h, const char *path)
 {
     if (!h || !path) return NNP_ERR_ARG;
+    const std::string hp = host_params(const_cast<nnp_handle *>(h)->E);
+    if (!hp.empty()) return fail(const_cast<nnp_handle *>(h), NNP_ERR_CUDA, hp);
     std::ofstream f(path, std::ios::out | std::ios::binary);
     if (!f) return fail(const_cast<nnp_handle *>(h), NNP_ERR_IO, std::string("NNP::write(const char*,const NNP&): Could not write to nnh file: \"") + path + "\"");
     f << nnp::write_potential(h->E.host);
@@ -628,6 +689,8 @@ int nnp_nparams(const nnp_handle *h, int32_t type, int32_t *n)
 int nnp_get_params(const nnp_handle *h, double *params)
 {
     if (!h || !params) return NNP_ERR_ARG;
+    const std::string hp = host_params(const_cast<nnp_handle *>(h)->E);
+    if (!hp.empty()) return fail(const_cast<nnp_handle *>(h), NNP_ERR_CUDA, hp);
     size_t k = 0;
     for (const auto &net : h->E.host.nets) {
         const int nl = (int)net.nodes.size() - 1;
@@ -645,6 +708,7 @@ int nnp_get_params(const nnp_handle *h, double *params)
 int nnp_set_params(nnp_handle *h, const double *params)
 {
     if (!h || !params) return NNP_ERR_ARG;
+    h->E.host_stale = false;          // every parameter is overwritten here
     size_t k = 0;
     for (auto &net : h->E.host.nets) {
         const int nl = (int)net.nodes.size() - 1;
@@ -980,6 +1044,8 @@ int nnp_precondition(nnp_handle *h, const nnp_batch *batch, int32_t prebias, int
     if (prescale < NNP_PRESCALE_IDENTITY || prescale > NNP_PRESCALE_MAX)
         return fail(h, NNP_ERR_ARG, "Invalid input scaling.");
     nnp::Engine &E = h->E;
+    const std::string hp = host_params(E);
+    if (!hp.empty()) return fail(h, NNP_ERR_CUDA, hp);
     const int T = E.host.ntypes(), gs = E.gstride;
     std::vector<int64_t> cnt(T);
     std::vector<double> st((size_t)T * NNP_NSTATS * gs);
@@ -1207,42 +1273,7 @@ int nnp_launch_count(const nnp_handle *h, int64_t *n)
     return NNP_OK;
 }
 
-namespace {
-int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta);
 
-// wpar offset of every network parameter in the reference packing (per type
-// in index order: biases by layer, then the weights column-major,
-// nn.cpp:881-915), and whether it is a weight
-void pack_offsets(const nnp::Engine &E, std::vector<int64_t> &idx, std::vector<unsigned char> *is_weight)
-{
-    idx.clear();
-    if (is_weight) is_weight->clear();
-    for (int t = 0; t < E.dpot.ntypes; ++t) {
-        const nnp::DevType &T = E.dpot.t[t];
-        const int nin = T.nodes[0], nout = T.nodes[T.nlayer];
-        int64_t off = T.woff + 2 * nin + 2 * nout;
-        std::vector<int64_t> boff(T.nlayer), woff(T.nlayer);
-        for (int l = 0; l < T.nlayer; ++l) {
-            boff[l] = off;
-            woff[l] = off + T.nodes[l + 1];
-            off = woff[l] + (int64_t)T.nodes[l] * nnp::wt_stride(T.nodes[l + 1]);
-        }
-        for (int l = 0; l < T.nlayer; ++l)
-            for (int n = 0; n < T.nodes[l + 1]; ++n) {
-                idx.push_back(boff[l] + n);
-                if (is_weight) is_weight->push_back(0);
-            }
-        for (int l = 0; l < T.nlayer; ++l) {
-            const int ni = T.nodes[l], no = T.nodes[l + 1], st = nnp::wt_stride(no);
-            for (int m = 0; m < ni; ++m)
-                for (int n = 0; n < no; ++n) {
-                    idx.push_back(woff[l] + (int64_t)m * st + n);
-                    if (is_weight) is_weight->push_back(1);
-                }
-        }
-    }
-}
-}  // namespace
 
 int nnp_opt_adam(nnp_handle *h, double gamma, double eps)
 {
@@ -1336,23 +1367,8 @@ int opt_adam_impl(nnp_handle *h, double gamma, double eps, int reg, double eta)
     }
     std::string msg = nnp::run_adam(E, gamma, eps, reg, eta);
     if (!msg.empty()) return fail(h, NNP_ERR_CUDA, msg);
-    // mirror the new parameters into the host model (nnp_get_params, nnp_write)
-    std::vector<double> val(E.adam_idx_host.size());
-    chk(cudaMemcpyAsync(val.data(), E.adam_p.p, sizeof(double) * val.size(), cudaMemcpyDeviceToHost, E.stream));
-    chk(cudaStreamSynchronize(E.stream));
-    if (ce != cudaSuccess) return fail(h, NNP_ERR_CUDA, std::string("ADAM step failed: ") + cudaGetErrorString(ce));
-    size_t k = 0;
-    for (auto &net : E.host.nets) {
-        const int nl = (int)net.nodes.size() - 1;
-        for (int l = 0; l < nl; ++l)
-            for (auto &v : net.b[l]) v = val[k++];
-        for (int l = 0; l < nl; ++l) {
-            const int ni = net.nodes[l], no = net.nodes[l + 1];
-            for (int m = 0; m < ni; ++m)
-                for (int n = 0; n < no; ++n) net.w[l][(size_t)n * ni + m] = val[k++];
-        }
-    }
-    for (size_t i = 0; i < E.adam_idx_host.size(); ++i) E.wpar_host[E.adam_idx_host[i]] = (float)val[i];
+    // the host model is brought up to date when it is next read (host_params)
+    E.host_stale = true;
     E.grad_valid = false;
     return NNP_OK;
 }

@@ -148,6 +148,7 @@ struct Engine {
     DBuf<unsigned char> adam_wmask;   // 1 for a weight, 0 for a bias (the weight-decay mask)
     double adam_b1i = 0.9, adam_b2i = 0.999;
     bool adam_master_stale = true;  // the master copy must be reloaded from the host model
+    bool host_stale = false;        // the host model lags the master copy (device optimiser steps)
     int loss_kind = 1;            // energy-loss kind of nnp_train_grad (NNP_LOSS_*)
     double loss_delta = 1.0;      // its width (HUBER, ASINH)
     float *noalloc_e_atom = nullptr;  // device address of the allocation-free call's scratch (looked up once)
