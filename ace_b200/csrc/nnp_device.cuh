@@ -612,30 +612,58 @@ __device__ __forceinline__ int small_div(int p, int m)
 //    n*floor((n-1)/2) + (n even ? n/2 : 0) = n(n-1)/2 pairs.
 // Lanes step p by 32, which is (q32, r32) = (32/m, 32%m) in (g, f): two
 // adds and one wrap per step instead of a division or a square root.
-// The force kernel stores per-pair coefficients chunk by chunk: a chunk is
-// NNP_FORCE_CHUNK consecutive pairs, pair p at coefficient index p - c0
-// (J != K rows may be split between chunks).
+// For J != K the larger segment gives the rows (the angular functions are
+// symmetric in the two neighbours), so a chunk's row owners and column owners
+// fit one pass of the force kernel's slot pass.
+// The force kernel stores per-pair coefficients chunk by chunk, a chunk being
+// whole rows [g0, g1): pair (g, f) at coefficient index (g - g0) s + f, with
+// the row stride s = n (J == K) or nb rounded up to an odd number (J != K),
+// so that row owners reading their rows side by side hit distinct banks.
 struct Blk {
-    int sa, na;       // first member: segment start / size
-    int sb, nb;       // second member (sb == sa for J == K)
+    int sa, na;       // first member (rows): segment start / size
+    int sb, nb;       // second member (columns; sb == sa for J == K)
     bool tri;
     int npairs;
     int m, q32, r32;
+    int rows, s;      // rows of pairs (J == K: n/2 with the half row), coefficient row stride
 };
 
 __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
 {
-    k.sa = v.seg[J];
-    k.na = v.seg[J + 1] - k.sa;
+    const int s0 = v.seg[J], n0 = v.seg[J + 1] - s0;
     k.tri = (J == K);
-    k.sb = k.tri ? k.sa : v.seg[K];
-    k.nb = k.tri ? k.na : v.seg[K + 1] - v.seg[K];
-    k.npairs = k.tri ? k.na * (k.na - 1) / 2 : k.na * k.nb;
+    if (k.tri) {
+        k.sa = k.sb = s0;
+        k.na = k.nb = n0;
+        k.npairs = n0 * (n0 - 1) / 2;
+        k.rows = n0 >> 1;
+        k.s = n0;
+    } else {
+        const int s1 = v.seg[K], n1 = v.seg[K + 1] - s1;
+        const bool sw = n1 > n0;
+        k.sa = sw ? s1 : s0;
+        k.na = sw ? n1 : n0;
+        k.sb = sw ? s0 : s1;
+        k.nb = sw ? n0 : n1;
+        k.npairs = k.na * k.nb;
+        k.rows = k.na;
+        k.s = k.nb | 1;
+    }
     if (k.npairs == 0) return false;
     k.m = k.nb;
     k.q32 = small_div(32, k.m);
     k.r32 = 32 - k.q32 * k.m;
     return true;
+}
+
+// rows of one coefficient chunk of the force kernel: as many as NNP_FORCE_CHUNK
+// coefficients hold, and for J != K with fewer than 32 columns at most
+// 32 - nb, so that rows and columns have one lane each in the slot pass
+__device__ __forceinline__ int chunk_rows(const Blk &k)
+{
+    int R = small_div(NNP_FORCE_CHUNK, k.s);
+    if (!k.tri && k.nb < 32) R = min(R, 32 - k.nb);
+    return max(R, 1);
 }
 
 struct PairIt {
@@ -754,10 +782,11 @@ __device__ __forceinline__ void pair_coeffs(float *pc, int q, float hc, float hr
     pc[2 * NNP_PCH + q] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
 }
 
-// Pair pass of the force kernel for pairs [c0,c1) of one block (any form):
+// Pair pass of the force kernel for pairs [c0,c1) of one block (any form),
+// whole rows, coefficients at it.g s + it.f - qoff:
 // dE/dcos, dE/dr_a, dE/dr_b from e = dE/dG of the block's functions.
-__device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B, const Blk &k, int c0, int c1, int cap,
-                                    int lane)
+__device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B, const Blk &k, int c0, int c1,
+                                           int qoff, int cap, int lane)
 {
     const float *eb = v.vec + B.off_g;
     const bool gauss = (B.form == ANG_GAUSS);
@@ -813,17 +842,17 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 hrb = fmaf(ef, drb, hrb);
             }
         }
-        pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);
+        pair_coeffs(v.pc, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);
     }
 }
 
-// Slot pass: each lane owns neighbour slots of the block (for J == K blocks of
-// at most 16 slots, one of the two halves of a slot's pairs) and sums, in a
-// fixed order, the coefficients of the pairs [c0,c1) that contain them.  With the numbering of Blk, slot x of a J == K
-// block is the first member of the pairs (x, x+s mod n) at p = (s-1)n + x and
-// the second member of the pairs (x-s mod n, x) at p = (s-1)n + (x-s mod n),
-// s = 1..(n-1)/2, plus s = n/2 for even n (first member if x < n/2, second
-// member otherwise).
+// Slot pass over the rows [g0, g1) of one chunk: each lane owns neighbour
+// slots of the block (for J == K blocks of at most 16 slots, one of the two
+// halves of a slot's pairs) and sums, in a fixed order, the coefficients of
+// the chunk's pairs that contain them.  With the numbering of Blk, slot x of
+// a J == K block is the first member of pair (x, x+g+1 mod n) and the second
+// member of pair (x-g-1 mod n, x) in row g; on the half row of an even n only
+// first members below n/2 have a pair.
 
 // g += sa u + (1/r) v for the slot with unit vector and 1/r us
 __device__ __forceinline__ void slot_add(const NbrView &v, int slot, float4 us, float sa_, float vx, float vy, float vz)
@@ -833,43 +862,51 @@ __device__ __forceinline__ void slot_add(const NbrView &v, int slot, float4 us, 
     v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
 }
 
-// J == K: the pair of row g in which slot x is the first (second == false) or
-// the second member, if it lies in the chunk
-__device__ __forceinline__ void tri_half(const NbrView &v, const Blk &k, const float *cS, const float *cH, int n,
-                                         int h, int x, bool second, int g, int c0, int c1, float &sa_, float &vx,
-                                         float &vy, float &vz)
+// J == K: slot x's pairs in rows [g0, g1) in which it is the first (second ==
+// false) or the second member; cS is the coefficient on its own unit vector.
+// The partner o and the coefficient index (g - g0) n + (first member) advance
+// by one row per step.
+__device__ __forceinline__ void tri_visits(const NbrView &v, const Blk &k, const float *cS, const float *cH, int x,
+                                           bool second, int g0, int g1, float &sa_, float &vx, float &vy, float &vz)
 {
-    const bool on = g != h || (second ? x >= (n >> 1) : x < (n >> 1));   // even n: half row g = n/2-1
-    int o = second ? x - g - 1 : x + g + 1;                              // partner
-    o = (o < 0) ? o + n : (o >= n ? o - n : o);
-    const int p = g * n + (second ? o : x);
-    if (on && p >= c0 && p < c1) {
-        const float4 uo = v.u[k.sa + o];
-        sa_ += cS[p - c0];
-        const float t = cH[p - c0];
-        vx = fmaf(t, uo.x, vx);
-        vy = fmaf(t, uo.y, vy);
-        vz = fmaf(t, uo.z, vz);
+    const int n = k.m, hn = n >> 1, hr = (n & 1) ? -1 : hn - 1;   // half row of an even n
+    int o = second ? x - g0 - 1 : x + g0 + 1;
+    o += (o < 0) ? n : 0;
+    o -= (o >= n) ? n : 0;
+    int base = 0;
+#pragma unroll 1
+    for (int g = g0; g < g1; ++g) {
+        const int first = second ? o : x;
+        if (g != hr || first < hn) {
+            const int q = base + first;
+            const float4 uo = v.u[k.sa + o];
+            sa_ += cS[q];
+            const float t = cH[q];
+            vx = fmaf(t, uo.x, vx);
+            vy = fmaf(t, uo.y, vy);
+            vz = fmaf(t, uo.z, vz);
+        }
+        base += n;
+        if (second) {
+            o = (o == 0) ? n - 1 : o - 1;
+        } else {
+            o = (o == n - 1) ? 0 : o + 1;
+        }
     }
 }
 
-__device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c1, int lane)
+__device__ inline void force_slots(const NbrView &v, const Blk &k, int g0, int g1, int lane)
 {
     const float *cA = v.pc, *cH = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH;
     if (k.tri) {
-        const int n = k.m, h = (n - 1) >> 1;
-        const int gmin = small_div(c0, n), gmax = min(small_div(c1 - 1, n), (n >> 1) - 1);   // rows g touching the chunk
+        const int n = k.m;
         if (n <= 16) {
             // lane x sums slot x's first-member pairs, lane n + x its
             // second-member pairs; the halves meet by a shuffle
             const bool second = lane >= n;
             const int x = second ? lane - n : lane;
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-            if (lane < 2 * n) {
-#pragma unroll 1
-                for (int g = gmin; g <= gmax; ++g)
-                    tri_half(v, k, second ? cC : cA, cH, n, h, x, second, g, c0, c1, sa_, vx, vy, vz);
-            }
+            if (lane < 2 * n) tri_visits(v, k, second ? cC : cA, cH, x, second, g0, g1, sa_, vx, vy, vz);
             sa_ += __shfl_down_sync(NNP_FULL, sa_, n);
             vx += __shfl_down_sync(NNP_FULL, vx, n);
             vy += __shfl_down_sync(NNP_FULL, vy, n);
@@ -879,38 +916,28 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
         }
         for (int x = lane; x < n; x += 32) {
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-#pragma unroll 1
-            for (int g = gmin; g <= gmax; ++g) {
-                tri_half(v, k, cA, cH, n, h, x, false, g, c0, c1, sa_, vx, vy, vz);
-                tri_half(v, k, cC, cH, n, h, x, true, g, c0, c1, sa_, vx, vy, vz);
-            }
+            tri_visits(v, k, cA, cH, x, false, g0, g1, sa_, vx, vy, vz);
+            tri_visits(v, k, cC, cH, x, true, g0, g1, sa_, vx, vy, vz);
             slot_add(v, k.sa + x, v.u[k.sa + x], sa_, vx, vy, vz);
         }
         return;
     }
-    // J != K: pair p = g * nb + f couples first member sa + g with second
-    // member sb + f.  A row owner reads the run of its row inside the chunk
-    // (stride 1), a column owner one entry per row (stride nb; row owners
-    // read with stride nb across lanes, column owners consecutively).  Row and
-    // column owners run the same loop (no divergent branches): slot sl walks
-    // its j-th pair with coefficient stride qs.
-    const int nslots = k.na + k.nb;
+    // J != K: pair (g, f) at (g - g0) s + f couples row slot sa + g with
+    // column slot sb + f.  A row owner reads its row (stride 1; row owners
+    // side by side at the odd stride s), a column owner one entry per row
+    // (stride s; column owners side by side).  Row and column owners run the
+    // same loop: slot sl walks its j-th pair at coefficient stride qs.
+    const int nr = g1 - g0, nslots = nr + k.nb;
     for (int sl = lane; sl < nslots; sl += 32) {
-        const bool is_row = sl < k.na;                 // first member of its pairs
-        const int slot = is_row ? k.sa + sl : k.sb + (sl - k.na);
+        const bool is_row = sl < nr;
+        const int slot = is_row ? k.sa + g0 + sl : k.sb + (sl - nr);
         const float4 us = v.u[slot];
-        float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        // row g = sl: pairs [max(c0, g nb), min(c1, (g+1) nb))
-        const int pb = sl * k.nb, lo = max(c0, pb), hi = min(c1, pb + k.nb);
-        // column f: rows glo .. ghi-1 with c0 <= g nb + f < c1
-        const int f = sl - k.na;
-        const int glo = c0 > f ? small_div(c0 - f + k.nb - 1, k.nb) : 0,
-                  ghi = c1 > f ? small_div(c1 - 1 - f, k.nb) + 1 : 0;
-        const int cnt = is_row ? hi - lo : ghi - glo;
-        const int q0 = is_row ? lo - c0 : glo * k.nb + f - c0;
-        const int qs = is_row ? 1 : k.nb;
+        const int cnt = is_row ? k.nb : nr;
+        const int q0 = is_row ? sl * k.s : sl - nr;
+        const int qs = is_row ? 1 : k.s;
         const float *c1p = is_row ? cA : cC;
-        const float4 *up = v.u + (is_row ? k.sb + (lo - pb) : k.sa + glo);
+        const float4 *up = v.u + (is_row ? k.sb : k.sa + g0);
+        float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
 #pragma unroll 2
         for (int j = 0; j < cnt; ++j) {
             const int q = q0 + j * qs;
@@ -921,9 +948,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int c0, int c
             vy = fmaf(bt, uo.y, vy);
             vz = fmaf(bt, uo.z, vz);
         }
-        v.gx[slot] += fmaf(sa_, us.x, us.w * vx);
-        v.gy[slot] += fmaf(sa_, us.y, us.w * vy);
-        v.gz[slot] += fmaf(sa_, us.z, us.w * vz);
+        slot_add(v, slot, us, sa_, vx, vy, vz);
     }
 }
 
@@ -960,7 +985,7 @@ struct GenericBlocks {
     template <typename Acc>
     // Gb: the block's first symmetry function in the atom's row; eb: its first dE/dG
     __device__ static bool symm(const NbrView &, int, int, const Blk &, int, int, float *) { return false; }
-    __device__ static bool force(const NbrView &, int, int, const Blk &, int, int, int, int, const float *)
+    __device__ static bool force(const NbrView &, int, int, const Blk &, int, int, int, int, int, const float *)
     {
         return false;
     }
@@ -1101,18 +1126,20 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             Blk k;
             if (!make_blk(v, J, K, k)) continue;
             bool staged = false;
-            for (int c0 = 0; c0 < k.npairs; c0 += NNP_FORCE_CHUNK) {
-                const int c1 = min(k.npairs, c0 + NNP_FORCE_CHUNK);
-                if (!Blocks::force(v, II, tt, k, c0, c1, cap, lane, v.vec + B.off_g)) {
+            const int R = chunk_rows(k);
+            for (int g0 = 0; g0 < k.rows; g0 += R) {
+                const int g1 = min(k.rows, g0 + R);
+                const int c0 = g0 * k.m, c1 = min(k.npairs, g1 * k.m), qoff = g0 * k.s;
+                if (!Blocks::force(v, II, tt, k, c0, c1, qoff, cap, lane, v.vec + B.off_g)) {
                     if (!staged) {
                         for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
                         __syncwarp();
                         staged = true;
                     }
-                    force_pairs_generic(v, B, k, c0, c1, cap, lane);
+                    force_pairs_generic(v, B, k, c0, c1, qoff, cap, lane);
                 }
                 __syncwarp();
-                force_slots(v, k, c0, c1, lane);
+                force_slots(v, k, g0, g1, lane);
                 __syncwarp();
             }
         }

@@ -217,7 +217,8 @@ std::string gen_symm_body(const Engine &E, const DevBlockA &B)
 }
 
 // Pair pass of one GAUSS block (see force_pairs_generic), relative to the
-// block's first dE/dG (eb).
+// block's first dE/dG (eb); coefficients of pair (g, f) at g s + f - qoff
+// (qoff: no generated local may take a parameter's name).
 std::string gen_force_body(const Engine &E, const DevBlockA &B)
 {
     std::ostringstream os;
@@ -261,7 +262,7 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
         body << "              hra = fmaf(gsp, da" << d << " * wb" << d << ", hra);\n";
         body << "              hrb = fmaf(gsp, wa" << d << " * db" << d << ", hrb); }\n";
     }
-    body << "            pair_coeffs(v.pc, p - c0, hc, hra, hrb, cs, ua.w, ub.w);\n";
+    body << "            pair_coeffs(v.pc, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);\n";
     os << body.str() << "            }\n            return true;\n        }\n";
     return os.str();
 }
@@ -392,8 +393,8 @@ std::string make_source(const Engine &E, const TuneParams &tp)
           "    __device__ static bool symm(const NbrView &v, int II, int tt, const Blk &k, int cap, int lane, float *Gb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
        << group_cases(sy) << "        default: return false;\n        }\n    }\n";
-    os << "    __device__ static bool force(const NbrView &v, int II, int tt, const Blk &k, int c0, int c1, int cap,\n"
-          "                                 int lane, const float *eb)\n"
+    os << "    __device__ static bool force(const NbrView &v, int II, int tt, const Blk &k, int c0, int c1, int qoff,\n"
+          "                                 int cap, int lane, const float *eb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
        << group_cases(fo) << "        default: return false;\n        }\n    }\n";
     os << "    __device__ static bool radial_force(int II, int t, float r, float fc, float fcd, const float *eb, float &out)\n"

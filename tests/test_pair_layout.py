@@ -1,94 +1,163 @@
-"""CPU checks of the index arithmetic that the force kernel's slot pass uses
-(ace_b200/csrc/nnp_device.cuh: Blk, PairIt, tri_half, force_slots, small_div),
-restated here in Python: for every chunking of a block's pairs, each pair is
-summed exactly once by the owner of its first slot and once by the owner of
-its second slot, at the coefficient index the pair pass wrote it to.  The GPU
-tests run the kernels themselves (forced small chunks, dense neighbour lists);
-these pin the enumeration for many block shapes in a second."""
+"""CPU checks of the index arithmetic that the force kernel's pair and slot
+passes use (ace_b200/csrc/nnp_device.cuh: make_blk, chunk_rows, PairIt,
+force_pairs_generic's coefficient index, tri_visits, force_slots, small_div),
+restated here in Python with the device code's integer steps: for every
+block shape up to the staging capacity and the chunk sizes the tuner may
+pick, the pair pass writes each pair of a chunk to a distinct coefficient
+inside the chunk's area, and the slot pass sums each pair exactly once for
+its first and once for its second slot, reading the coefficient the pair
+pass wrote it to.  The GPU tests run the kernels themselves; these pin the
+enumeration for all block shapes in seconds."""
 import numpy as np
 import pytest
 
+NNP_PCH = 288
+CAPACITY = 256
 
-def tri_pairs(n):
-    """Pair numbering of a J == K block of n slots: p = g n + f couples slot f
-    with slot (f + g + 1) mod n for g < (n-1)/2, plus the half row g = n/2-1,
-    f < n/2, for even n."""
+
+def small_div(p, m):
+    assert 0 <= p < (1 << 22) and 1 <= m <= 1024
+    return p // m
+
+
+def make_blk(n0, n1, tri):
+    """Blk of a block whose J segment starts at slot 0 and K segment at n0"""
+    if tri:
+        k = dict(sa=0, na=n0, sb=0, nb=n0, tri=True, npairs=n0 * (n0 - 1) // 2, rows=n0 >> 1, s=n0)
+    else:
+        s0, s1 = 0, n0
+        if n1 > n0:
+            k = dict(sa=s1, na=n1, sb=s0, nb=n0)
+        else:
+            k = dict(sa=s0, na=n0, sb=s1, nb=n1)
+        k.update(tri=False, npairs=k["na"] * k["nb"], rows=k["na"], s=k["nb"] | 1)
+    if k["npairs"] == 0:
+        return None
+    k["m"] = k["nb"]
+    k["q32"] = small_div(32, k["m"])
+    k["r32"] = 32 - k["q32"] * k["m"]
+    return k
+
+
+def chunk_rows(k, chunk):
+    R = small_div(chunk, k["s"])
+    if not k["tri"] and k["nb"] < 32:
+        R = min(R, 32 - k["nb"])
+    return max(R, 1)
+
+
+def pair_pass(k, c0, c1, q0):
+    """(coefficient index, first slot, second slot) of the pairs [c0, c1), as
+    the lanes' PairIt walks them (p = lane + 32 t)"""
     out = []
-    h = (n - 1) // 2
-    for g in range(h):
-        out += [(f, (f + g + 1) % n) for f in range(n)]
-    if n % 2 == 0 and n >= 2:
-        g = n // 2 - 1
-        out += [(f, (f + g + 1) % n) for f in range(n // 2)]
+    for lane in range(32):
+        p = c0 + lane
+        g = small_div(p, k["m"])
+        f = p - g * k["m"]
+        while p < c1:
+            if k["tri"]:
+                bb = f + g + 1
+                a, b = k["sa"] + f, k["sa"] + (bb - k["m"] if bb >= k["m"] else bb)
+            else:
+                a, b = k["sa"] + g, k["sb"] + f
+            out.append((g * k["s"] + f - q0, a, b))
+            p += 32
+            f += k["r32"]
+            g += k["q32"]
+            if f >= k["m"]:
+                f -= k["m"]
+                g += 1
     return out
 
 
-def tri_half(n, x, second, g, c0, c1):
-    """Pair index (or None) of row g in which slot x is the first or second member."""
-    h = (n - 1) >> 1
-    on = g != h or (x >= (n >> 1) if second else x < (n >> 1))
-    o = x - g - 1 if second else x + g + 1
-    o = o + n if o < 0 else (o - n if o >= n else o)
-    p = g * n + (o if second else x)
-    return p if (on and c0 <= p < c1) else None
+def tri_visits(k, x, second, g0, g1):
+    """(coefficient index, partner) of slot x's pairs in rows [g0, g1)"""
+    n = k["m"]
+    hn, hr = n >> 1, (-1 if n & 1 else (n >> 1) - 1)
+    o = x - g0 - 1 if second else x + g0 + 1
+    o += n if o < 0 else 0
+    o -= n if o >= n else 0
+    base, out = 0, []
+    for g in range(g0, g1):
+        first = o if second else x
+        if g != hr or first < hn:
+            out.append((base + first, k["sa"] + o))
+        base += n
+        o = (n - 1 if o == 0 else o - 1) if second else (0 if o == n - 1 else o + 1)
+    return out
 
 
-@pytest.mark.parametrize("chunk", [7, 32, 256])
-def test_tri_slots_cover_every_pair_twice(chunk):
-    for n in range(2, 70):
-        pairs = tri_pairs(n)
-        assert len(pairs) == n * (n - 1) // 2
-        assert len({tuple(sorted(q)) for q in pairs}) == len(pairs)      # every unordered pair once
-        got = {x: [] for x in range(n)}
-        for c0 in range(0, len(pairs), chunk):
-            c1 = min(len(pairs), c0 + chunk)
-            gmin, gmax = c0 // n, min((c1 - 1) // n, (n >> 1) - 1)
-            for x in range(n):
-                for g in range(gmin, gmax + 1):
-                    for second in (False, True):
-                        p = tri_half(n, x, second, g, c0, c1)
-                        if p is not None:
-                            a, b = pairs[p]
-                            assert (b if second else a) == x
-                            got[x].append(p)
-        for x in range(n):
-            assert sorted(got[x]) == [p for p, q in enumerate(pairs) if x in q]
+def slot_pass(k, g0, g1):
+    """slot -> list of (coefficient index, side, partner): side 'A' = the
+    slot is the pair's first member (cA), 'C' = second member (cC)"""
+    got = {}
+    if k["tri"]:
+        for x in range(k["m"]):
+            for second in (False, True):
+                for q, o in tri_visits(k, x, second, g0, g1):
+                    got.setdefault(k["sa"] + x, []).append((q, "C" if second else "A", o))
+        return got
+    nr = g1 - g0
+    for sl in range(nr + k["nb"]):
+        is_row = sl < nr
+        slot = k["sa"] + g0 + sl if is_row else k["sb"] + (sl - nr)
+        cnt = k["nb"] if is_row else nr
+        q0 = sl * k["s"] if is_row else sl - nr
+        qs = 1 if is_row else k["s"]
+        up = k["sb"] if is_row else k["sa"] + g0
+        for j in range(cnt):
+            got.setdefault(slot, []).append((q0 + j * qs, "A" if is_row else "C", up + j))
+    return got
 
 
-@pytest.mark.parametrize("chunk", [7, 32, 256])
-def test_rect_slots_cover_every_pair_twice(chunk):
-    """J != K: pair p = g nb + f; a row owner reads its row's run inside the
-    chunk, a column owner one entry per row (rows may be split by chunks)."""
-    for na in list(range(1, 18)) + [40]:
-        for nb in list(range(1, 18)) + [33, 200, 255]:
-            npairs = na * nb
-            rows, cols = {}, {}
-            for c0 in range(0, npairs, chunk):
-                c1 = min(npairs, c0 + chunk)
-                for sl in range(na + nb):
-                    is_row = sl < na
-                    pb = sl * nb
-                    lo, hi = max(c0, pb), min(c1, pb + nb)
-                    f = sl - na
-                    glo = -(-(c0 - f) // nb) if c0 > f else 0
-                    ghi = (c1 - 1 - f) // nb + 1 if c1 > f else 0
-                    cnt = hi - lo if is_row else ghi - glo
-                    q0 = lo - c0 if is_row else glo * nb + f - c0
-                    qs = 1 if is_row else nb
-                    for j in range(max(cnt, 0)):
-                        q = q0 + j * qs
-                        assert 0 <= q < c1 - c0
-                        g, ff = divmod(c0 + q, nb)
-                        if is_row:
-                            assert g == sl
-                            rows.setdefault(sl, []).append(c0 + q)
-                        else:
-                            assert ff == f
-                            cols.setdefault(f, []).append(c0 + q)
-            for g in range(na):
-                assert sorted(rows[g]) == [g * nb + f for f in range(nb)]
-            for f in range(nb):
-                assert sorted(cols[f]) == [g * nb + f for g in range(na)]
+def check(n0, n1, tri, chunk):
+    k = make_blk(n0, n1, tri)
+    if tri:
+        want = {frozenset((a, b)) for a in range(n0) for b in range(a + 1, n0)}
+    else:
+        want = {frozenset((a, b)) for a in range(n0) for b in range(n0, n0 + n1)}
+    if k is None:
+        assert not want
+        return
+    if not tri:
+        assert k["na"] >= k["nb"] and k["s"] % 2 == 1                # larger segment as rows, odd stride
+    R = chunk_rows(k, chunk)
+    seen = []
+    for g0 in range(0, k["rows"], R):
+        g1 = min(k["rows"], g0 + R)
+        c0, c1, q0 = g0 * k["m"], min(k["npairs"], g1 * k["m"]), g0 * k["s"]
+        written = {}
+        for q, a, b in pair_pass(k, c0, c1, q0):
+            assert 0 <= q < NNP_PCH and q not in written          # inside the chunk area, once
+            written[q] = (a, b)
+            seen.append(frozenset((a, b)))
+        if not tri and k["nb"] < 32:
+            assert (g1 - g0) + k["nb"] <= 32                       # one lane per row and column
+        visits = {}
+        for slot, lst in slot_pass(k, g0, g1).items():
+            for q, side, partner in lst:
+                assert q in written                                 # reads what the pair pass wrote
+                a, b = written[q]
+                assert (a, b) == ((slot, partner) if side == "A" else (partner, slot))
+                visits[(q, side)] = visits.get((q, side), 0) + 1
+        assert all(c == 1 for c in visits.values())
+        assert len(visits) == 2 * len(written)                     # every pair once per member
+    assert len(seen) == len(want) and set(seen) == want
+
+
+@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 40])
+def test_tri_blocks(chunk):
+    for n in range(0, CAPACITY + 1, 1 if chunk == NNP_PCH else 5):
+        check(n, n, True, chunk)
+
+
+@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 40])
+def test_rect_blocks(chunk):
+    sizes = list(range(0, 34)) + [47, 64, 65, 100, 128, 200, 255]
+    for n0 in sizes[:: (1 if chunk == NNP_PCH else 3)]:
+        for n1 in sizes:
+            if n0 + n1 <= CAPACITY:
+                check(n0, n1, False, chunk)
 
 
 def test_small_div_correction():
