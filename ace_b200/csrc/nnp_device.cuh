@@ -457,7 +457,7 @@ struct NbrView {
     float *fc, *fd;     // cutoff value / slope [ncut][C]
     float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr, groups in pairs (wix)
     float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
-    float *vec;         // dE/dG row [gstride]
+    float *vec;         // dE/dG rows of the current and the next atom [2][gstride] (16-byte aligned)
     float *pc;          // pair coefficients [3][NNP_PCH]
     int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
     unsigned char *t;   // neighbour type [C]
@@ -466,7 +466,7 @@ struct NbrView {
 NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
 {
     return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 4 * ((ndamp + 1) / 2) * C +
-           (force ? 4 * C + 3 * C + gstride + 3 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+           (force ? 4 * C + 3 * C + 2 * gstride + 3 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
 __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
@@ -477,8 +477,10 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
     v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
     if (force) {
         v.raw = reinterpret_cast<float4 *>(p); p += 4 * C;           // stays 16-byte aligned
+        v.vec = p; p += 2 * gstride;                                  // gstride % 4 == 0
     } else {
         v.raw = nullptr;
+        v.vec = nullptr;
     }
     v.r = p; p += C;
     v.j = reinterpret_cast<int *>(p); p += C;
@@ -490,10 +492,9 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
         v.gx = p; p += C;
         v.gy = p; p += C;
         v.gz = p; p += C;
-        v.vec = p; p += gstride;
         v.pc = p; p += 3 * NNP_PCH;
     } else {
-        v.gx = v.gy = v.gz = v.vec = v.pc = nullptr;
+        v.gx = v.gy = v.gz = v.pc = nullptr;
     }
     v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
     v.t = reinterpret_cast<unsigned char *>(p);
@@ -577,6 +578,30 @@ __device__ __forceinline__ int stage_prefetched(const NbrView &v, int n, int cap
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncwarp();
     return stage_records(v, v.raw, n, cap, P, T, lane);
+}
+
+// The force kernel's atom walk is a load pipeline: while the warp works on
+// one atom, the records and the dE/dG row of the next stream into shared
+// memory (cp.async), and the neighbour count and type of the atom after that
+// and the index of the third load into registers, so that no global load of
+// the walk waits for another.  Count and type travel packed: n << 4 | type
+// (types at or above 15 read as 15, which no potential has).
+__device__ __forceinline__ int pack_nt(int n, int t) { return (n << 4) | (int)min((unsigned)t, 15u); }
+
+// cp.async of n neighbour records into raw and of the first nrow floats of a
+// dE/dG row (16-byte chunks; rows are gstride floats, gstride % 4 == 0)
+__device__ __forceinline__ void prefetch_rows(float4 *raw, const float4 *src, int n, float *vdst, const float *vsrc,
+                                              int nrow, int lane)
+{
+    for (int k = lane; k < n; k += 32) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(raw + k);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + k) : "memory");
+    }
+    for (int k = lane; 4 * k < nrow; k += 32) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(vdst + 4 * k);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(vsrc + 4 * k) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // Lanes of a radial block of n <= 32 functions: G phases per function (the
@@ -783,12 +808,11 @@ __device__ __forceinline__ void pair_coeffs(float *pc, int q, float hc, float hr
 }
 
 // Pair pass of the force kernel for pairs [c0,c1) of one block (any form),
-// whole rows, coefficients at it.g s + it.f - qoff:
+// whole rows, coefficients at it.g s + it.f - qoff, eb = dE/dG of the block:
 // dE/dcos, dE/dr_a, dE/dr_b from e = dE/dG of the block's functions.
-__device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B, const Blk &k, int c0, int c1,
-                                           int qoff, int cap, int lane)
+__device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B, const float *eb, const Blk &k, int c0,
+                                           int c1, int qoff, int cap, int lane)
 {
-    const float *eb = v.vec + B.off_g;
     const bool gauss = (B.form == ANG_GAUSS);
     PairIt it = pit_init(k, c0 + lane);
 #pragma unroll 1
@@ -1080,24 +1104,43 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
     const DevPot &P = *pot;
     const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;
-    i64 i_next = 0;
-    int n_next = 0;
-    prefetch_atom(v, idx0, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
-    for (i64 idx = idx0; idx < N; idx += stride) {
-        const i64 i = i_next;
-        const int II = type[i];
-        if ((unsigned)II >= (unsigned)P.ntypes) {               // type out of range (reported by the call)
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-            __syncwarp();
-            prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
-            continue;
-        }
-        const DevType &T = P.t[II];
-        const int n = stage_prefetched(v, n_next, cap, P, T, lane);
-        prefetch_atom(v, idx + stride, N, order, nbr, nbr_cnt, cap, lane, i_next, n_next);
-        const float *e = dEdG + i * gstride;
-        for (int g = lane; g < T.n_input; g += 32) v.vec[g] = e[g];
+    // load pipeline (pack_nt): atom idx (i0, nt0) is in shared memory, atom
+    // idx + stride (i1, nt1) known, atom idx + 2 stride (i2) indexed
+    auto row_len = [&](int nt) { return ((nt & 15) < P.ntypes) ? P.t[nt & 15].n_input : 0; };
+    int i0 = 0, nt0 = 0, i1 = 0, nt1 = 0, i2 = 0;
+    if (idx0 < N) {
+        i0 = order[idx0];
+        nt0 = pack_nt(nbr_cnt[i0], type[i0]);
+        prefetch_rows(v.raw, nbr + (i64)i0 * cap, nt0 >> 4, v.vec, dEdG + (i64)i0 * gstride, row_len(nt0), lane);
+    }
+    if (idx0 + stride < N) {
+        i1 = order[idx0 + stride];
+        nt1 = pack_nt(nbr_cnt[i1], type[i1]);
+    }
+    if (idx0 + 2 * stride < N) i2 = order[idx0 + 2 * stride];
+    int buf = 0;
+    for (i64 idx = idx0; idx < N; idx += stride, buf ^= 1) {
+        const i64 i = i0;
+        const int II = nt0 & 15;
+        // loads for two and three atoms on, used by later iterations
+        const int nt2 = (idx + 2 * stride < N) ? pack_nt(nbr_cnt[i2], type[i2]) : 0;
+        const int i3 = (idx + 3 * stride < N) ? order[idx + 3 * stride] : 0;
+        const float *vc = v.vec + buf * gstride;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncwarp();
+        const bool ok = II < P.ntypes;                          // else type out of range (reported by the call)
+        const int n = ok ? stage_records(v, v.raw, nt0 >> 4, cap, P, P.t[II], lane) : 0;
+        // the next atom's records and dE/dG row stream in meanwhile
+        if (idx + stride < N)
+            prefetch_rows(v.raw, nbr + (i64)i1 * cap, nt1 >> 4, v.vec + (buf ^ 1) * gstride,
+                          dEdG + (i64)i1 * gstride, row_len(nt1), lane);
+        i0 = i1;
+        nt0 = nt1;
+        i1 = i2;
+        nt1 = nt2;
+        i2 = i3;
+        if (!ok) continue;
+        const DevType &T = P.t[II];
         // radial: lanes own their neighbour slot (initialises g)
         for (int k = lane; k < n; k += 32) {
             const int tk = v.t[k];
@@ -1105,12 +1148,12 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             const float4 u = v.u[k];
             const float fc = v.fc[B.cut * cap + k], fd = v.fd[B.cut * cap + k];
             float amp = 0.f;
-            if (!Blocks::radial_force(II, tk, v.r[k], fc, fd, v.vec + B.off_g, amp)) {
+            if (!Blocks::radial_force(II, tk, v.r[k], fc, fd, vc + B.off_g, amp)) {
                 for (int f = 0; f < B.n; ++f) {
                     const float2 q = rpar[B.par + f];
                     float val, der;
                     radial_fd(B.form, v.r[k], q.x, q.y, fc, fd, val, der);
-                    amp = fmaf(v.vec[B.off_g + f], der, amp);
+                    amp = fmaf(vc[B.off_g + f], der, amp);
                 }
             }
             v.gx[k] = amp * u.x;
@@ -1130,13 +1173,13 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             for (int g0 = 0; g0 < k.rows; g0 += R) {
                 const int g1 = min(k.rows, g0 + R);
                 const int c0 = g0 * k.m, c1 = min(k.npairs, g1 * k.m), qoff = g0 * k.s;
-                if (!Blocks::force(v, II, tt, k, c0, c1, qoff, cap, lane, v.vec + B.off_g)) {
+                if (!Blocks::force(v, II, tt, k, c0, c1, qoff, cap, lane, vc + B.off_g)) {
                     if (!staged) {
                         for (int f = lane; f < B.n; f += 32) v.par[f] = apar[B.par + f];
                         __syncwarp();
                         staged = true;
                     }
-                    force_pairs_generic(v, B, k, c0, c1, qoff, cap, lane);
+                    force_pairs_generic(v, B, vc + B.off_g, k, c0, c1, qoff, cap, lane);
                 }
                 __syncwarp();
                 force_slots(v, k, g0, g1, lane);
