@@ -184,15 +184,25 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return None
+        lines = open(self.path).read().splitlines() if os.path.exists(self.path) else []
+        if not lines:
+            # a region shorter than the sampling period: one reading at its end
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10)
+                lines = r.stdout.splitlines()
+            except Exception:
+                lines = []
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.fh.close()
+        lines += [x for x in open(self.path).read().splitlines() if x not in lines]
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
