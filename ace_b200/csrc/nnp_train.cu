@@ -17,6 +17,8 @@
 //   k_nn_train  warp per atom: network forward with its tangent along C_i,
 //               reverse pass over both, parameter gradients summed per block
 //               in shared memory and added to an FP64 global gradient.
+#include <cstdlib>
+
 #include "nnp_device.cuh"
 #include "nnp_engine.h"
 
@@ -158,6 +160,215 @@ k_nn_train(i64 N, const DevPot *__restrict__ pot, const float *__restrict__ wpar
     }
 }
 
+// ---------------------------------------------------------------- tiled weight gradient
+//
+// k_nn_train_tile: the same gradient as k_nn_train for tiles of TT_ROWS atoms
+// of one element.  Lane r of every warp is atom r of the tile; the warps
+// split each layer's columns.  Forward (primal and tangent) and reverse are
+// small matrix products over the tile in shared memory, arrays column-major
+// with row stride TT_LD so that lanes (atoms) and threads walking columns hit
+// distinct banks.  The weight gradient of a layer, sum over the tile's atoms
+// of zb x^T + zbt xt^T, is one thread per entry; the bias gradient one warp
+// sum per column.  Both add into a gradient copy of the element's network in
+// shared memory (no atomics: every entry has one owner per phase), which is
+// added to the FP64 global gradient when the CTA moves on to another element
+// and at its end.
+#define TT_ROWS 32
+#define TT_LD 33
+
+// floats of one element's network in wpar (the layout of net_view)
+__host__ __device__ inline int net_floats(const DevType &T)
+{
+    int n = 2 * T.nodes[0] + 2 * T.nodes[T.nlayer];
+    for (int l = 0; l < T.nlayer; ++l) n += T.nodes[l + 1] + T.nodes[l] * wt_stride(T.nodes[l + 1]);
+    return n;
+}
+
+struct TrainTileDims {
+    int maxw;      // floats of the largest element network, rounded up to 4
+    int maxin;     // widest input layer
+    int sumout;    // largest sum of layer widths nodes[1..L] of one element
+    int maxn;      // widest layer
+};
+
+__host__ __device__ inline size_t train_tile_floats(const TrainTileDims &d)
+{
+    return 2 * (size_t)d.maxw + (size_t)TT_LD * (2 * d.maxin + 5 * d.sumout + 4 * d.maxn);
+}
+
+__global__ void __launch_bounds__(WARPS * 32)
+k_nn_train_tile(const DevPot *__restrict__ pot, const float *__restrict__ wpar, const int *__restrict__ type_count,
+                const int *__restrict__ order, const float *__restrict__ G, const float *__restrict__ C, int gstride,
+                const float *__restrict__ gE, double *__restrict__ grad, TrainTileDims dims)
+{
+    extern __shared__ float smem[];
+    const DevPot &P = *pot;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, r = lane;
+    int first[NNP_MAX_TYPES + 1], base[NNP_MAX_TYPES + 1];
+    first[0] = 0;
+    base[0] = 0;
+    for (int T = 0; T < P.ntypes; ++T) {
+        const int c = type_count[T];
+        first[T + 1] = first[T] + (c + TT_ROWS - 1) / TT_ROWS;
+        base[T + 1] = base[T] + c;
+    }
+    const int ntiles = first[P.ntypes];
+    float *w_s = smem, *g_s = smem + dims.maxw;
+    float *ins = g_s + dims.maxw, *inst = ins + TT_LD * dims.maxin;
+    float *lay = inst + TT_LD * dims.maxin;                   // per layer A, D, D2, ZT, AT [no][TT_LD]
+    float *ab = lay + 5 * TT_LD * dims.sumout, *abt = ab + TT_LD * dims.maxn, *nab = abt + TT_LD * dims.maxn,
+          *nabt = nab + TT_LD * dims.maxn;
+    const bool tan = (C != nullptr);
+    int cur = -1, cur_n = 0;
+    auto flush = [&]() {                                       // gradient copy -> FP64 global gradient
+        __syncthreads();
+        double *gd = grad + P.t[cur].woff;
+        for (int k = t; k < cur_n; k += blockDim.x) {
+            const float g = g_s[k];
+            if (g != 0.f) atomicAdd(gd + k, (double)g);
+        }
+        __syncthreads();
+    };
+    for (int g = blockIdx.x; g < ntiles; g += gridDim.x) {
+        int T = 0;
+        while (g >= first[T + 1]) ++T;
+        const DevType &DT = P.t[T];
+        if (T != cur) {
+            if (cur >= 0) flush();
+            cur = T;
+            cur_n = net_floats(DT);
+            for (int k = t; k < cur_n; k += blockDim.x) {
+                w_s[k] = wpar[DT.woff + k];
+                g_s[k] = 0.f;
+            }
+            __syncthreads();
+        }
+        const NetView Vw = net_view(w_s, DT);
+        const int L = DT.nlayer, nin = DT.nodes[0], nout = DT.nodes[L];
+        const int j0 = (g - first[T]) * TT_ROWS, cnt = type_count[T];
+        // inputs, scaled: warp w loads atoms w, w + 8, ..., lanes over the row
+        for (int rr = warp; rr < TT_ROWS; rr += WARPS) {
+            const bool lv = j0 + rr < cnt;
+            const i64 ir = lv ? order[base[T] + j0 + rr] : 0;
+            for (int m = lane; m < nin; m += 32) {
+                ins[m * TT_LD + rr] = lv ? Vw.inpw[m] * (G[ir * gstride + m] + Vw.inpb[m]) : 0.f;
+                inst[m * TT_LD + rr] = (lv && tan) ? Vw.inpw[m] * C[ir * gstride + m] : 0.f;
+            }
+        }
+        __syncthreads();
+        const bool live = j0 + r < cnt;
+        // forward, primal and tangent; columns n = warp + 8k, four at a time
+        float *la = lay;
+        for (int l = 0; l < L; ++l) {
+            const int ni = DT.nodes[l], no = DT.nodes[l + 1], s = Vw.ws[l];
+            const int neu = (l == L - 1) ? NEU_LINEAR : DT.neuron;
+            const float *x = (l == 0) ? ins : la - 5 * TT_LD * ni;   // A and AT of the previous layer
+            const float *xt = (l == 0) ? inst : la - TT_LD * ni;
+            float *A = la, *D = A + TT_LD * no, *D2 = D + TT_LD * no, *ZT = D2 + TT_LD * no, *AT = ZT + TT_LD * no;
+            for (int n0 = warp; n0 < no; n0 += 4 * WARPS) {
+                float z[4], zt[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int n = n0 + k * WARPS;
+                    z[k] = (n < no) ? Vw.b[l][n] : 0.f;
+                    zt[k] = 0.f;
+                }
+                for (int m = 0; m < ni; ++m) {
+                    const float xv = x[m * TT_LD + r], xtv = xt[m * TT_LD + r];
+                    const float *wr = Vw.wt[l] + m * s;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int n = n0 + k * WARPS;
+                        const float w = (n < no) ? wr[n] : 0.f;
+                        z[k] = fmaf(w, xv, z[k]);
+                        zt[k] = fmaf(w, xtv, zt[k]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int n = n0 + k * WARPS;
+                    if (n < no) {
+                        float a, d, d2;
+                        activation(neu, DT.c, z[k], a, d, d2);
+                        A[n * TT_LD + r] = a;
+                        D[n * TT_LD + r] = d;
+                        D2[n * TT_LD + r] = d2;
+                        ZT[n * TT_LD + r] = zt[k];
+                        AT[n * TT_LD + r] = d * zt[k];
+                    }
+                }
+            }
+            la += 5 * TT_LD * no;
+            __syncthreads();
+        }
+        // reverse seeds: phi = gE E_i - (dE_i/dG) . C_i
+        {
+            const float ge = live ? gE[order[base[T] + j0 + r]] : 0.f;
+            for (int n = warp; n < nout; n += WARPS) {
+                ab[n * TT_LD + r] = ge * Vw.outw[n];
+                abt[n * TT_LD + r] = (live && tan) ? -Vw.outw[n] : 0.f;
+            }
+        }
+        __syncthreads();
+        float *gb = g_s + 2 * nin + 2 * nout;                   // this layer's bias gradient (walks the layout)
+        float *glb[NNP_MAX_LAYERS];
+        for (int l = 0; l < L; ++l) {
+            glb[l] = gb;
+            gb += DT.nodes[l + 1] + DT.nodes[l] * Vw.ws[l];
+        }
+        float *cab = ab, *cabt = abt, *cnab = nab, *cnabt = nabt;
+        for (int l = L - 1; l >= 0; --l) {
+            const int ni = DT.nodes[l], no = DT.nodes[l + 1], s = Vw.ws[l];
+            la -= 5 * TT_LD * no;
+            const float *D = la + TT_LD * no, *D2 = D + TT_LD * no, *ZT = D2 + TT_LD * no;
+            const float *x = (l == 0) ? ins : la - 5 * TT_LD * ni;
+            const float *xt = (l == 0) ? inst : la - TT_LD * ni;
+            // zb, zbt in place of the adjoint; bias gradient by warp sums
+            for (int n = warp; n < no; n += WARPS) {
+                const int q = n * TT_LD + r;
+                const float d = D[q];
+                const float zb = fmaf(cab[q], d, cabt[q] * D2[q] * ZT[q]);
+                cabt[q] = cabt[q] * d;
+                cab[q] = zb;
+                const float sb = warp_sum(zb);
+                if (lane == 0) glb[l][n] += sb;
+            }
+            __syncthreads();
+            // weight gradient: entry (m, n) = sum over atoms of zb_n x_m + zbt_n xt_m
+            float *gw = glb[l] + no;
+            for (int e = t; e < ni * no; e += blockDim.x) {
+                const int m = e / no, n = e - m * no;
+                const float *zr = cab + n * TT_LD, *ztr = cabt + n * TT_LD;
+                const float *xr = x + m * TT_LD, *xtr = xt + m * TT_LD;
+                float acc = 0.f;
+#pragma unroll 8
+                for (int a = 0; a < TT_ROWS; ++a) acc = fmaf(zr[a], xr[a], fmaf(ztr[a], xtr[a], acc));
+                gw[m * s + n] += acc;
+            }
+            // adjoint of the layer input: W^T zb
+            if (l > 0) {
+                for (int m = warp; m < ni; m += WARPS) {
+                    const float *wr = Vw.wt[l] + m * s;
+                    float a = 0.f, at = 0.f;
+                    for (int n = 0; n < no; ++n) {
+                        a = fmaf(wr[n], cab[n * TT_LD + r], a);
+                        at = fmaf(wr[n], cabt[n * TT_LD + r], at);
+                    }
+                    cnab[m * TT_LD + r] = a;
+                    cnabt[m * TT_LD + r] = at;
+                }
+            }
+            __syncthreads();
+            float *s1 = cab, *s2 = cabt;
+            cab = cnab;
+            cabt = cnabt;
+            cnab = s1;
+            cnabt = s2;
+        }
+    }
+    if (cur >= 0) flush();
+}
+
 static int grid_for(int64_t items, int per_block, int max_blocks)
 {
     int64_t b = (items + per_block - 1) / per_block;
@@ -209,6 +420,30 @@ std::string run_train_grad(Engine &E, bool with_force)
             std::string msg = cuda_msg("tangent symmetry functions");
             if (!msg.empty()) return msg;
         }
+    }
+    // tiles of one element's atoms when their arrays fit in shared memory
+    // (NNP_TRAIN_TILE=0 selects the warp-per-atom kernel)
+    TrainTileDims dims{1, 1, 1, 1};
+    for (int t = 0; t < E.dpot.ntypes; ++t) {
+        const DevType &T = E.dpot.t[t];
+        int so = 0;
+        for (int l = 0; l < T.nlayer; ++l) so += T.nodes[l + 1];
+        dims.maxw = std::max(dims.maxw, (net_floats(T) + 3) & ~3);
+        dims.maxin = std::max(dims.maxin, T.nodes[0]);
+        dims.sumout = std::max(dims.sumout, so);
+        for (int l = 0; l <= T.nlayer; ++l) dims.maxn = std::max(dims.maxn, T.nodes[l]);
+    }
+    const size_t smt = train_tile_floats(dims) * sizeof(float);
+    const char *tile_env = std::getenv("NNP_TRAIN_TILE");
+    if (smt <= 227 * 1024 && !(tile_env && tile_env[0] == '0')) {
+        cudaFuncSetAttribute(k_nn_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (smt + 1024))));
+        const int grid = grid_for(N / TT_ROWS + E.dpot.ntypes, 1, nsm * per_sm);
+        k_nn_train_tile<<<grid, WARPS * 32, smt, E.stream>>>(E.d_pot, E.wpar.p, E.type_fill.p, E.order.p, E.G.p,
+                                                            with_force ? E.tang.p : nullptr, E.gstride, E.gE.p,
+                                                            E.pgrad.p, dims);
+        E.launches += 1;
+        return cuda_msg("k_nn_train_tile");
     }
     const size_t sm = (size_t)(2 * ((E.wfloats + 3) & ~3) + WARPS * train_warp_floats(maxl, maxn)) * sizeof(float);
     if (sm > 227 * 1024) return "networks too large for the shared-memory training kernel";

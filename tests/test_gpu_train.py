@@ -263,3 +263,22 @@ def test_device_pointer_training_matches_host(tmp_path):
         gamma = nn.opt_step(gamma, t, "EXP", 1e-3, 0, "NONE", 0.0)
     nn.close()
     assert losses[-1] < 0.7 * losses[0]
+
+
+@pytest.mark.parametrize("w_f", [0.0, 0.5])
+def test_tiled_gradient_matches_warp_kernel(tmp_path, monkeypatch, w_f):
+    """The tiled network-gradient kernel (tiles of 32 atoms of one element,
+    the default when its arrays fit in shared memory) gives the warp-per-atom
+    kernel's gradient (NNP_TRAIN_TILE=0) to FP32 summation order, on a batch
+    of 600+ atoms whose tiles of two elements are shared out over the CTAs."""
+    b, path, e_ref, f_ref = setup(tmp_path, n=14, seed=57)
+    assert b.n_atoms > 500
+    nn = NNP.read(path)
+    L1, g1, _, _ = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, w_f, norm_mode=1)
+    nn.close()
+    monkeypatch.setenv("NNP_TRAIN_TILE", "0")
+    nn = NNP.read(path)
+    L0, g0, _, _ = nn.train_grad(b.atom_off, b.pos, b.type, b.cell, e_ref, f_ref, w_f, norm_mode=1)
+    nn.close()
+    assert abs(L1 - L0) <= 1e-12 * abs(L0)
+    assert np.abs(g1 - g0).max() <= 1e-5 * np.abs(g0).max()
