@@ -310,21 +310,30 @@ __device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
     return (unsigned)atom | (tt << 28);
 }
 
-// one thread per cell (all structures): insertion sort of the cell's member
-// list by (type, atom index), so the neighbour order does not depend on the
-// order of the atomic insertions, and the count of each type among the
-// members.  Lists of up to 64 members are sorted in a local copy.
-__global__ void k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
-                             const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
-                             const int *__restrict__ type, int ntypes, int *__restrict__ cell_atoms,
-                             int *__restrict__ cell_tcnt)
+// The members of every cell (all structures) sorted by (type, atom index)
+// and counted per type.  A lane sorts a cell of at most 64 atoms in registers
+// (insertion sort); the warp then ranks its larger cells together, one at a
+// time: the keys type << 28 | atom are distinct, so a key's place is the
+// number of smaller keys (the same order as any comparison sort), each lane
+// ranking four of its keys per load of a compared key.  Those keys sit in the
+// warp's shared memory, or for a cell of more than SORT_SMEM atoms (a free
+// structure of up to NNP_FREE_ONE_CELL atoms is one cell) in tmp at the
+// cell's own slots.
+#define SORT_WARPS 4
+#define SORT_SMEM 512
+__global__ void __launch_bounds__(SORT_WARPS * 32)
+k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
+             const int *__restrict__ cell_cnt, const int *__restrict__ cell_start, const int *__restrict__ type,
+             int ntypes, int *__restrict__ cell_atoms, int *__restrict__ cell_tcnt, unsigned *__restrict__ tmp)
 {
+    __shared__ unsigned keys[SORT_WARPS][SORT_SMEM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= grid[S - 1].cell_base + ncells[S - 1]) return;
-    int *a = cell_atoms + cell_start[c];
-    const int n = cell_cnt[c];
-    int *tc = cell_tcnt + (size_t)c * ntypes;
-    if (n <= 64) {
+    const bool valid = c < grid[S - 1].cell_base + ncells[S - 1];
+    const int n = valid ? cell_cnt[c] : 0;
+    if (valid && n <= 64) {
+        int *a = cell_atoms + cell_start[c];
+        int *tc = cell_tcnt + (size_t)c * ntypes;
         int key[64];
         for (int p = 0; p < n; ++p) {
             const unsigned v = sort_key(a[p], type[a[p]], ntypes);
@@ -340,29 +349,45 @@ __global__ void k_sort_cells(int S, const StructGrid *__restrict__ grid, const i
             p = q;
         }
         for (; p < n; ++p) a[p] = key[p] & 0x0fffffff;          // out-of-range types, last
-        return;
     }
-    unsigned *u = reinterpret_cast<unsigned *>(a);
-    for (int p = 0; p < n; ++p) u[p] = sort_key(a[p], type[a[p]], ntypes);
-    for (int p = 1; p < n; ++p) {
-        const unsigned v = u[p];
-        int q = p - 1;
-        while (q >= 0 && u[q] > v) { u[q + 1] = u[q]; --q; }
-        u[q + 1] = v;
+    unsigned big = __ballot_sync(0xffffffffu, valid && n > 64);
+    while (big) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int cc = __shfl_sync(0xffffffffu, c, src), nn = __shfl_sync(0xffffffffu, n, src);
+        int *a = cell_atoms + cell_start[cc];
+        unsigned *k = (nn <= SORT_SMEM) ? keys[warp] : tmp + cell_start[cc];
+        for (int p = lane; p < nn; p += 32) k[p] = sort_key(a[p], type[a[p]], ntypes);
+        __threadfence_block();
+        __syncwarp();
+        for (int p0 = lane; p0 < nn; p0 += 128) {
+            unsigned v[4];
+            int r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] = (p0 + 32 * u < nn) ? k[p0 + 32 * u] : 0xffffffffu;
+                r[u] = 0;
+            }
+            for (int q = 0; q < nn; ++q) {
+                const unsigned w = k[q];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) r[u] += (w < v[u]) ? 1 : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (p0 + 32 * u < nn) a[r[u]] = (int)(v[u] & 0x0fffffffu);
+        }
+        for (int t = 0; t < ntypes; ++t) {
+            int m = 0;
+            for (int p = lane; p < nn; p += 32) m += ((k[p] >> 28) == (unsigned)t) ? 1 : 0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+            if (lane == 0) cell_tcnt[(size_t)cc * ntypes + t] = m;
+        }
+        __syncwarp();                                            // keys[warp] reused by the next cell
     }
-    int p = 0;
-    for (int t = 0; t < ntypes; ++t) {
-        int q = p;
-        while (q < n && (u[q] >> 28) == (unsigned)t) ++q;
-        tc[t] = q - p;
-        p = q;
-    }
-    for (int q = 0; q < n; ++q) u[q] &= 0x0fffffffu;
 }
 
-// cell-ordered copy of the wrapped positions with the atom's type in .w (-1
-// for a type outside [0, ntypes): such atoms are never neighbours), so the
-// neighbour search reads each cell's members contiguously
 __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const double *__restrict__ xw,
                            const int *__restrict__ type, int ntypes, double4 *__restrict__ cell_pos)
 {
@@ -1136,8 +1161,10 @@ std::string run_neighbors(Engine &E, int pbc)
                                                      E.cell_cnt.p);
     k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
-    k_sort_cells<<<grid_for((int64_t)cell_bound, 128, 1 << 30), 128, 0, st>>>(
-        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes, E.cell_atoms.p, E.cell_tcnt.p);
+    // (atom_cell, read only by k_fill, holds the keys of the largest cells)
+    k_sort_cells<<<grid_for((int64_t)cell_bound, SORT_WARPS * 32, 1 << 30), SORT_WARPS * 32, 0, st>>>(
+        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes, E.cell_atoms.p, E.cell_tcnt.p,
+        reinterpret_cast<unsigned *>(E.atom_cell.p));
     k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
                                                           E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
