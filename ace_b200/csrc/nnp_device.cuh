@@ -24,9 +24,9 @@
 
 #define NNP_WARPS 8           // warps per block of the per-atom kernels
 #define NNP_SYMM_CHUNK 8      // angular functions accumulated in registers per pass
-#define NNP_PCH 288           // pair coefficients the force kernel stores per chunk
+#define NNP_PCH 288           // default pair coefficients of one force-kernel chunk
 #ifndef NNP_FORCE_CHUNK
-#define NNP_FORCE_CHUNK NNP_PCH   // pairs per chunk of the force kernel (<= NNP_PCH)
+#define NNP_FORCE_CHUNK NNP_PCH   // pair coefficients of one chunk of this build's force kernel (<= NNP_PCH)
 #endif
 #define NNP_FULL 0xffffffffu
 
@@ -458,15 +458,21 @@ struct NbrView {
     float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr, groups in pairs (wix)
     float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
     float *vec;         // dE/dG rows of the current and the next atom [2][gstride] (16-byte aligned)
-    float *pc;          // pair coefficients [3][NNP_PCH]
+    float *pc;          // pair coefficients [3][pcs]
+    int pcs;            // their array length: the chunk, at least one row (C)
     int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
     unsigned char *t;   // neighbour type [C]
 };
 
-NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force)
+// length of each pair-coefficient array of a force view: the chunk the
+// kernel was built for, and never less than one row (C slots), so that a
+// smaller chunk frees shared memory for resident blocks
+NNP_HD inline int coef_len(int chunk, int C) { return chunk > C ? chunk : C; }
+
+NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force, int chunk)
 {
     return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 4 * ((ndamp + 1) / 2) * C +
-           (force ? 4 * C + 3 * C + 2 * gstride + 3 * NNP_PCH : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+           (force ? 4 * C + 3 * C + 2 * gstride + 3 * coef_len(chunk, C) : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
 __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
@@ -492,8 +498,10 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
         v.gx = p; p += C;
         v.gy = p; p += C;
         v.gz = p; p += C;
-        v.pc = p; p += 3 * NNP_PCH;
+        v.pcs = coef_len(NNP_FORCE_CHUNK, C);
+        v.pc = p; p += 3 * v.pcs;
     } else {
+        v.pcs = 0;
         v.gx = v.gy = v.gz = v.pc = nullptr;
     }
     v.seg = reinterpret_cast<int *>(p); p += NNP_MAX_TYPES + 1;
@@ -686,7 +694,7 @@ __device__ __forceinline__ bool make_blk(const NbrView &v, int J, int K, Blk &k)
 // 32 - nb, so that rows and columns have one lane each in the slot pass
 __device__ __forceinline__ int chunk_rows(const Blk &k)
 {
-    int R = small_div(NNP_FORCE_CHUNK, k.s);
+    int R = small_div(NNP_FORCE_CHUNK, k.s);   // R s <= chunk, or R = 1 and s <= cap <= pcs
     if (!k.tri && k.nb < 32) R = min(R, 32 - k.nb);
     return max(R, 1);
 }
@@ -799,12 +807,12 @@ __device__ void symm_block_generic(const NbrView &v, const DevBlockA &B, const B
 
 // Writes the three dE/dd coefficients of one pair (see force_body); ira, irb
 // are the inverse distances.
-__device__ __forceinline__ void pair_coeffs(float *pc, int q, float hc, float hra, float hrb, float cs, float ira,
-                                            float irb)
+__device__ __forceinline__ void pair_coeffs(float *pc, int pcs, int q, float hc, float hra, float hrb, float cs,
+                                            float ira, float irb)
 {
     pc[q] = hra - hc * cs * ira;                 // on u_a in dE/dd_a
-    pc[NNP_PCH + q] = hc;                        // on u_b / r_a in dE/dd_a, on u_a / r_b in dE/dd_b
-    pc[2 * NNP_PCH + q] = hrb - hc * cs * irb;   // on u_b in dE/dd_b
+    pc[pcs + q] = hc;                            // on u_b / r_a in dE/dd_a, on u_a / r_b in dE/dd_b
+    pc[2 * pcs + q] = hrb - hc * cs * irb;       // on u_b in dE/dd_b
 }
 
 // Pair pass of the force kernel for pairs [c0,c1) of one block (any form),
@@ -866,7 +874,7 @@ __device__ inline void force_pairs_generic(const NbrView &v, const DevBlockA &B,
                 hrb = fmaf(ef, drb, hrb);
             }
         }
-        pair_coeffs(v.pc, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);
+        pair_coeffs(v.pc, v.pcs, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);
     }
 }
 
@@ -921,7 +929,7 @@ __device__ __forceinline__ void tri_visits(const NbrView &v, const Blk &k, const
 
 __device__ inline void force_slots(const NbrView &v, const Blk &k, int g0, int g1, int lane)
 {
-    const float *cA = v.pc, *cH = v.pc + NNP_PCH, *cC = v.pc + 2 * NNP_PCH;
+    const float *cA = v.pc, *cH = v.pc + v.pcs, *cC = v.pc + 2 * v.pcs;
     if (k.tri) {
         const int n = k.m;
         if (n <= 16) {
@@ -1033,7 +1041,7 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
                           int ndamp_max, int gstride, float *__restrict__ G, float *smem)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, false);
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, false, NNP_FORCE_CHUNK);
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, false);
     const DevPot &P = *pot;
     for (i64 idx = blockIdx.x * (i64)NNP_WARPS + warp; idx < N; idx += (i64)gridDim.x * NNP_WARPS) {
@@ -1100,7 +1108,7 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
                            double *__restrict__ vir = nullptr)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true, NNP_FORCE_CHUNK);
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
     const DevPot &P = *pot;
     const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;
@@ -1249,11 +1257,11 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
                              float *smem)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true);
+    const int per = nbr_view_floats(cap, ncut_max, ndamp_max, gstride, true, NNP_FORCE_CHUNK);
     const NbrView v = nbr_view(smem + (size_t)warp * ((per + 3) & ~3), cap, ncut_max, ndamp_max, gstride, true);
     // the force view's per-neighbour gradient arrays hold the relative
     // displacement dv_k = V_i - V_k, and its pair-coefficient area the rate
-    // of change of the distance, rr_k = u_k . dv_k (cap <= NNP_MAX_NBR <= 3 NNP_PCH)
+    // of change of the distance, rr_k = u_k . dv_k (cap <= 3 pcs)
     float *rr = v.pc;
     const DevPot &P = *pot;
     const i64 stride = (i64)gridDim.x * NNP_WARPS, idx0 = blockIdx.x * (i64)NNP_WARPS + warp;

@@ -54,7 +54,7 @@ struct TuneParams {
     int symm_minb = 4;          // blocks per SM the specialised symmetry-function kernel's registers are budgeted for (1..4)
     int force_minb = 1;         // the same for the specialised force kernel (1..4)
     int force_unroll = 1;       // unroll factor of the specialised force kernel's pair loop (1..4)
-    int force_chunk = NNP_PCH;  // pairs per coefficient chunk of the force kernel (8..NNP_PCH)
+    int force_chunk = NNP_PCH;  // pair coefficients per chunk of the force kernel (8..NNP_PCH); sets its shared memory
     int tc_per_sm = 0;          // CTAs per SM of the tensor-core network kernel (0: as many as fit, at most 4)
     bool operator==(const TuneParams &o) const
     {

@@ -262,7 +262,7 @@ std::string gen_force_body(const Engine &E, const DevBlockA &B)
         body << "              hra = fmaf(gsp, da" << d << " * wb" << d << ", hra);\n";
         body << "              hrb = fmaf(gsp, wa" << d << " * db" << d << ", hrb); }\n";
     }
-    body << "            pair_coeffs(v.pc, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);\n";
+    body << "            pair_coeffs(v.pc, v.pcs, it.g * k.s + it.f - qoff, hc, hra, hrb, cs, ua.w, ub.w);\n";
     os << body.str() << "            }\n            return true;\n        }\n";
     return os.str();
 }

@@ -1093,9 +1093,12 @@ static int ndamp_max(const Engine &E)
     return m;
 }
 
-static size_t view_bytes(const Engine &E, bool force)
+// shared memory of the per-atom kernels; the force view's coefficient arrays
+// follow the chunk of the kernel launched (the specialised one's tuned chunk)
+static size_t view_bytes(const Engine &E, bool force, bool jit)
 {
-    const int per = nbr_view_floats(E.cap, ncut_max(E), ndamp_max(E), E.gstride, force);
+    const int per = nbr_view_floats(E.cap, ncut_max(E), ndamp_max(E), E.gstride, force,
+                                    jit ? E.tune.force_chunk : NNP_PCH);
     return (size_t)WARPS * ((per + 3) & ~3) * sizeof(float);
 }
 
@@ -1181,7 +1184,7 @@ std::string run_symm(Engine &E)
 {
     const int64_t N = E.n_centre;      // centres: the first n_centre entries of `order`
     if (N == 0) return "";
-    const size_t sm = view_bytes(E, false);
+    const size_t sm = view_bytes(E, false, false);
     const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
     if (E.use_jit && E.jit_symm && !E.acc64 && !E.symm64) {
@@ -1243,7 +1246,7 @@ std::string run_force(Engine &E)
     cudaMemsetAsync(E.force.p, 0, 3 * (size_t)E.n_atoms * sizeof(double), E.stream);
     double *vir = E.want_virial ? E.vir.p : nullptr;
     if (vir) cudaMemsetAsync(vir, 0, 9 * (size_t)E.n_struct * sizeof(double), E.stream);
-    const size_t sm = view_bytes(E, true);
+    const size_t sm = view_bytes(E, true, E.use_jit && E.jit_force);
     const int grid = grid_for(N, WARPS, num_sms() * 16);
     E.launches += 1;
     if (E.use_jit && E.jit_force) {

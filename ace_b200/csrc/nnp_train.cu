@@ -401,7 +401,8 @@ std::string run_train_grad(Engine &E, bool with_force)
     }
     maxn = (maxn + 3) & ~3;
     if (with_force) {
-        const int per = nbr_view_floats(E.cap, ncut, ndamp, E.gstride, true);
+        const int per = nbr_view_floats(E.cap, ncut, ndamp, E.gstride, true,
+                                        (E.use_jit && E.jit_tangent) ? E.tune.force_chunk : NNP_PCH);
         const size_t sm = (size_t)WARPS * ((per + 3) & ~3) * sizeof(float);
         if (sm > 227 * 1024) return "neighbour capacity too large for the tangent kernel";
         const int grid = grid_for(N, WARPS, nsm * 16);

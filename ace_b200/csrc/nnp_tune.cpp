@@ -43,7 +43,7 @@ namespace {
 // options only k_force_jit, the network option only k_nn_tc.
 struct ForceOpt { int minb, unroll, chunk; };
 const int kSymmMinb[] = {4, 3, 2};
-const ForceOpt kForce[] = {{1, 1, NNP_PCH}, {1, 2, NNP_PCH}, {2, 1, NNP_PCH}, {1, 1, 192}, {1, 1, 144}};
+const ForceOpt kForce[] = {{1, 1, NNP_PCH}, {2, 1, NNP_PCH}, {1, 1, 192}, {2, 1, 192}, {2, 1, 144}};
 const int kTcPerSm[] = {0, 1, 2, 3};
 constexpr int kCandidates = 5;
 constexpr int kReps = 3;        // timed repetitions per candidate (median)

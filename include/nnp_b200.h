@@ -141,8 +141,9 @@ int nnp_specialization_check(const char *potential_path, char *log, int32_t log_
  * longer.  Results do not depend on the choices beyond FP32 summation order.
  * Choices (params[0..4]): blocks per SM the symmetry-function kernel's
  * registers are budgeted for, the same for the force kernel, the force
- * kernel's pair-loop unroll, its pairs per coefficient chunk, and CTAs per
- * SM of the tensor-core network kernel (0 = as many as fit).
+ * kernel's pair-loop unroll, its pair coefficients per chunk (a smaller
+ * chunk needs less shared memory, so more blocks may be resident), and CTAs
+ * per SM of the tensor-core network kernel (0 = as many as fit).
  * nnp_tune_params returns the handle's current choices, where they came from
  * (*source: 0 defaults, 1 tuning cache, 2 tuned on this handle) and the last
  * tuning's measurements (*log).  nnp_tune_cache_key / _store / _load read and

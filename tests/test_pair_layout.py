@@ -6,13 +6,19 @@ block shape up to the staging capacity and the chunk sizes the tuner may
 pick, the pair pass writes each pair of a chunk to a distinct coefficient
 inside the chunk's area, and the slot pass sums each pair exactly once for
 its first and once for its second slot, reading the coefficient the pair
-pass wrote it to.  The GPU tests run the kernels themselves; these pin the
-enumeration for all block shapes in seconds."""
+pass wrote it to.  Coefficient indices stay below the per-array length
+coef_len(chunk, cap) = max(chunk, cap), checked at the smallest capacity a
+block can have (its own slots).  The GPU tests run the kernels themselves;
+these pin the enumeration for all block shapes in seconds."""
 import numpy as np
 import pytest
 
 NNP_PCH = 288
 CAPACITY = 256
+
+
+def coef_len(chunk, cap):
+    return max(chunk, cap)
 
 
 def small_div(p, m):
@@ -122,13 +128,14 @@ def check(n0, n1, tri, chunk):
     if not tri:
         assert k["na"] >= k["nb"] and k["s"] % 2 == 1                # larger segment as rows, odd stride
     R = chunk_rows(k, chunk)
+    area = coef_len(chunk, n0 if tri else n0 + n1)                  # smallest capacity holding the block
     seen = []
     for g0 in range(0, k["rows"], R):
         g1 = min(k["rows"], g0 + R)
         c0, c1, q0 = g0 * k["m"], min(k["npairs"], g1 * k["m"]), g0 * k["s"]
         written = {}
         for q, a, b in pair_pass(k, c0, c1, q0):
-            assert 0 <= q < NNP_PCH and q not in written          # inside the chunk area, once
+            assert 0 <= q < area and q not in written             # inside the coefficient arrays, once
             written[q] = (a, b)
             seen.append(frozenset((a, b)))
         if not tri and k["nb"] < 32:
@@ -145,13 +152,13 @@ def check(n0, n1, tri, chunk):
     assert len(seen) == len(want) and set(seen) == want
 
 
-@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 40])
+@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 144, 40, 7])
 def test_tri_blocks(chunk):
     for n in range(0, CAPACITY + 1, 1 if chunk == NNP_PCH else 5):
         check(n, n, True, chunk)
 
 
-@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 40])
+@pytest.mark.parametrize("chunk", [NNP_PCH, 192, 144, 40, 7])
 def test_rect_blocks(chunk):
     sizes = list(range(0, 34)) + [47, 64, 65, 100, 128, 200, 255]
     for n0 in sizes[:: (1 if chunk == NNP_PCH else 3)]:
