@@ -457,7 +457,7 @@ struct NbrView {
     float *fc, *fd;     // cutoff value / slope [ncut][C]
     float *w, *wd;      // GAUSS damping w_e(r) = fc exp(-a_e r^2) and dw_e/dr, groups in pairs (wix)
     float *gx, *gy, *gz;// per-slot gradient dE_i/dd_j [C]
-    float *vec;         // dE/dG rows of the current and the next atom [2][gstride] (16-byte aligned)
+    float *vec;         // dE/dG row of the atom [gstride] (16-byte aligned)
     float *pc;          // pair coefficients [3][pcs]
     int pcs;            // their array length: the chunk, at least one row (C)
     int *seg;           // [NNP_MAX_TYPES+1] type-segment starts
@@ -472,7 +472,7 @@ NNP_HD inline int coef_len(int chunk, int C) { return chunk > C ? chunk : C; }
 NNP_HD inline int nbr_view_floats(int C, int ncut, int ndamp, int gstride, bool force, int chunk)
 {
     return 4 * C + 4 * NNP_MAX_AFUNC + 2 * C + 2 * ncut * C + 4 * ((ndamp + 1) / 2) * C +
-           (force ? 4 * C + 3 * C + 2 * gstride + 3 * coef_len(chunk, C) : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
+           (force ? 4 * C + 3 * C + gstride + 3 * coef_len(chunk, C) : 0) + NNP_MAX_TYPES + 1 + (C + 3) / 4;
 }
 
 __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int gstride, bool force)
@@ -483,7 +483,7 @@ __device__ inline NbrView nbr_view(float *base, int C, int ncut, int ndamp, int 
     v.par = reinterpret_cast<float4 *>(p); p += 4 * NNP_MAX_AFUNC;
     if (force) {
         v.raw = reinterpret_cast<float4 *>(p); p += 4 * C;           // stays 16-byte aligned
-        v.vec = p; p += 2 * gstride;                                  // gstride % 4 == 0
+        v.vec = p; p += gstride;                                      // gstride % 4 == 0
     } else {
         v.raw = nullptr;
         v.vec = nullptr;
@@ -589,10 +589,13 @@ __device__ __forceinline__ int stage_prefetched(const NbrView &v, int n, int cap
 }
 
 // The force kernel's atom walk is a load pipeline: while the warp works on
-// one atom, the records and the dE/dG row of the next stream into shared
-// memory (cp.async), and the neighbour count and type of the atom after that
-// and the index of the third load into registers, so that no global load of
-// the walk waits for another.  Count and type travel packed: n << 4 | type
+// one atom, the records of the next stream into shared memory (cp.async),
+// then its dE/dG row once the atom's own row is no longer read (during the
+// scatter), and the neighbour count and type of the atom after that and the
+// index of the third load into registers, so that no global load of the walk
+// waits for another.  (A second row buffer would overlap the row with the
+// whole atom but costs the shared memory of a resident block at some
+// capacities.)  Count and type travel packed: n << 4 | type
 // (types at or above 15 read as 15, which no potential has).
 __device__ __forceinline__ int pack_nt(int n, int t) { return (n << 4) | (int)min((unsigned)t, 15u); }
 
@@ -1126,28 +1129,30 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
         nt1 = pack_nt(nbr_cnt[i1], type[i1]);
     }
     if (idx0 + 2 * stride < N) i2 = order[idx0 + 2 * stride];
-    int buf = 0;
-    for (i64 idx = idx0; idx < N; idx += stride, buf ^= 1) {
+    for (i64 idx = idx0; idx < N; idx += stride) {
         const i64 i = i0;
         const int II = nt0 & 15;
         // loads for two and three atoms on, used by later iterations
         const int nt2 = (idx + 2 * stride < N) ? pack_nt(nbr_cnt[i2], type[i2]) : 0;
         const int i3 = (idx + 3 * stride < N) ? order[idx + 3 * stride] : 0;
-        const float *vc = v.vec + buf * gstride;
+        const float *vc = v.vec;
         asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncwarp();
         const bool ok = II < P.ntypes;                          // else type out of range (reported by the call)
         const int n = ok ? stage_records(v, v.raw, nt0 >> 4, cap, P, P.t[II], lane) : 0;
         // the next atom's records and dE/dG row stream in meanwhile
-        if (idx + stride < N)
-            prefetch_rows(v.raw, nbr + (i64)i1 * cap, nt1 >> 4, v.vec + (buf ^ 1) * gstride,
-                          dEdG + (i64)i1 * gstride, row_len(nt1), lane);
+        const bool more = idx + stride < N;
+        const int in = i1, ntn = nt1;
+        if (more) prefetch_rows(v.raw, nbr + (i64)i1 * cap, nt1 >> 4, nullptr, nullptr, 0, lane);
         i0 = i1;
         nt0 = nt1;
         i1 = i2;
         nt1 = nt2;
         i2 = i3;
-        if (!ok) continue;
+        if (!ok) {
+            if (more) prefetch_rows(nullptr, nullptr, 0, v.vec, dEdG + (i64)in * gstride, row_len(ntn), lane);
+            continue;
+        }
         const DevType &T = P.t[II];
         // radial: lanes own their neighbour slot (initialises g)
         for (int k = lane; k < n; k += 32) {
@@ -1195,6 +1200,8 @@ __device__ void force_body(i64 N, const DevPot *__restrict__ pot, const float2 *
             }
         }
         __syncwarp();
+        // the next atom's dE/dG row streams in during the scatter
+        if (more) prefetch_rows(nullptr, nullptr, 0, v.vec, dEdG + (i64)in * gstride, row_len(ntn), lane);
         // scatter: F_j += g_j, F_i -= sum g_j
         double fx = 0.0, fy = 0.0, fz = 0.0;
         bool bad = false;
