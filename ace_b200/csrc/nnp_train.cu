@@ -334,16 +334,43 @@ k_nn_train_tile(const DevPot *__restrict__ pot, const float *__restrict__ wpar, 
                 if (lane == 0) glb[l][n] += sb;
             }
             __syncthreads();
-            // weight gradient: entry (m, n) = sum over atoms of zb_n x_m + zbt_n xt_m
+            // weight gradient: entry (m, n) = sum over atoms of zb_n x_m + zbt_n
+            // xt_m, a thread per block of 4 inputs x 2 outputs (12 loads per 16
+            // FMA; threads of a warp walk the outputs, so the x rows broadcast)
             float *gw = glb[l] + no;
-            for (int e = t; e < ni * no; e += blockDim.x) {
-                const int m = e / no, n = e - m * no;
-                const float *zr = cab + n * TT_LD, *ztr = cabt + n * TT_LD;
-                const float *xr = x + m * TT_LD, *xtr = xt + m * TT_LD;
-                float acc = 0.f;
-#pragma unroll 8
-                for (int a = 0; a < TT_ROWS; ++a) acc = fmaf(zr[a], xr[a], fmaf(ztr[a], xtr[a], acc));
-                gw[m * s + n] += acc;
+            const int nb2 = (no + 1) >> 1, nblk = ((ni + 3) >> 2) * nb2;
+            for (int e = t; e < nblk; e += blockDim.x) {
+                const int mb = e / nb2, m0 = 4 * mb, n0 = 2 * (e - mb * nb2);
+                const bool n1ok = n0 + 1 < no;
+                const float *z0 = cab + n0 * TT_LD, *zt0 = cabt + n0 * TT_LD;
+                const float *z1 = n1ok ? z0 + TT_LD : z0, *zt1 = n1ok ? zt0 + TT_LD : zt0;
+                const float *xr[4], *xtr[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int m = min(m0 + u, ni - 1);
+                    xr[u] = x + m * TT_LD;
+                    xtr[u] = xt + m * TT_LD;
+                }
+                float acc[4][2];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = 0.f;
+#pragma unroll 4
+                for (int a = 0; a < TT_ROWS; ++a) {
+                    const float za = z0[a], zta = zt0[a], zb1 = z1[a], ztb = zt1[a];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const float xv = xr[u][a], xtv = xtr[u][a];
+                        acc[u][0] = fmaf(za, xv, fmaf(zta, xtv, acc[u][0]));
+                        acc[u][1] = fmaf(zb1, xv, fmaf(ztb, xtv, acc[u][1]));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (m0 + u < ni) {
+                        gw[(m0 + u) * s + n0] += acc[u][0];
+                        if (n1ok) gw[(m0 + u) * s + n0 + 1] += acc[u][1];
+                    }
+                }
             }
             // adjoint of the layer input: W^T zb
             if (l > 0) {
