@@ -930,6 +930,51 @@ __device__ __forceinline__ void tri_visits(const NbrView &v, const Blk &k, const
     }
 }
 
+// J == K, both halves of slot x's pairs in rows [g0, g1) in one walk: pair
+// (x, of) with x first and pair (os, x) with x second, of advancing and os
+// retreating by one per row, each half in its own sums (two independent
+// chains), joined at the end
+__device__ __forceinline__ void tri_visits2(const NbrView &v, const Blk &k, const float *cA, const float *cH,
+                                            const float *cC, int x, int g0, int g1, float &sa_, float &vx, float &vy,
+                                            float &vz)
+{
+    const int n = k.m, hn = n >> 1, hr = (n & 1) ? -1 : hn - 1;   // half row of an even n
+    int of = x + g0 + 1, os = x - g0 - 1;
+    of -= (of >= n) ? n : 0;
+    os += (os < 0) ? n : 0;
+    float s2 = 0.f, wx = 0.f, wy = 0.f, wz = 0.f;
+    int base = 0;
+#pragma unroll 1
+    for (int g = g0; g < g1; ++g) {
+        const bool half = (g == hr);
+        if (!half || x < hn) {
+            const int q = base + x;
+            const float4 uo = v.u[k.sa + of];
+            sa_ += cA[q];
+            const float t = cH[q];
+            vx = fmaf(t, uo.x, vx);
+            vy = fmaf(t, uo.y, vy);
+            vz = fmaf(t, uo.z, vz);
+        }
+        if (!half || os < hn) {
+            const int q = base + os;
+            const float4 uo = v.u[k.sa + os];
+            s2 += cC[q];
+            const float t = cH[q];
+            wx = fmaf(t, uo.x, wx);
+            wy = fmaf(t, uo.y, wy);
+            wz = fmaf(t, uo.z, wz);
+        }
+        base += n;
+        of = (of == n - 1) ? 0 : of + 1;
+        os = (os == 0) ? n - 1 : os - 1;
+    }
+    sa_ += s2;
+    vx += wx;
+    vy += wy;
+    vz += wz;
+}
+
 __device__ inline void force_slots(const NbrView &v, const Blk &k, int g0, int g1, int lane)
 {
     const float *cA = v.pc, *cH = v.pc + v.pcs, *cC = v.pc + 2 * v.pcs;
@@ -951,8 +996,7 @@ __device__ inline void force_slots(const NbrView &v, const Blk &k, int g0, int g
         }
         for (int x = lane; x < n; x += 32) {
             float sa_ = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-            tri_visits(v, k, cA, cH, x, false, g0, g1, sa_, vx, vy, vz);
-            tri_visits(v, k, cC, cH, x, true, g0, g1, sa_, vx, vy, vz);
+            tri_visits2(v, k, cA, cH, cC, x, g0, g1, sa_, vx, vy, vz);
             slot_add(v, k.sa + x, v.u[k.sa + x], sa_, vx, vy, vz);
         }
         return;

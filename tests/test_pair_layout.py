@@ -1,6 +1,6 @@
 """CPU checks of the index arithmetic that the force kernel's pair and slot
 passes use (ace_b200/csrc/nnp_device.cuh: make_blk, chunk_rows, PairIt,
-force_pairs_generic's coefficient index, tri_visits, force_slots, small_div),
+force_pairs_generic's coefficient index, tri_visits, tri_visits2, force_slots, small_div),
 restated here in Python with the device code's integer steps: for every
 block shape up to the staging capacity and the chunk sizes the tuner may
 pick, the pair pass writes each pair of a chunk to a distinct coefficient
@@ -93,12 +93,36 @@ def tri_visits(k, x, second, g0, g1):
     return out
 
 
+def tri_visits2(k, x, g0, g1):
+    """tri_visits of both halves in one walk (J == K blocks of more than 16
+    slots): (coefficient index, side, partner) in walk order"""
+    n = k["m"]
+    hn, hr = n >> 1, (-1 if n & 1 else (n >> 1) - 1)
+    of, os = x + g0 + 1, x - g0 - 1
+    of -= n if of >= n else 0
+    os += n if os < 0 else 0
+    base, out = 0, []
+    for g in range(g0, g1):
+        half = g == hr
+        if not half or x < hn:
+            out.append((base + x, "A", k["sa"] + of))
+        if not half or os < hn:
+            out.append((base + os, "C", k["sa"] + os))
+        base += n
+        of = 0 if of == n - 1 else of + 1
+        os = n - 1 if os == 0 else os - 1
+    return out
+
+
 def slot_pass(k, g0, g1):
     """slot -> list of (coefficient index, side, partner): side 'A' = the
     slot is the pair's first member (cA), 'C' = second member (cC)"""
     got = {}
     if k["tri"]:
         for x in range(k["m"]):
+            if k["m"] > 16:                                   # one walk over both halves
+                got[k["sa"] + x] = tri_visits2(k, x, g0, g1)
+                continue
             for second in (False, True):
                 for q, o in tri_visits(k, x, second, g0, g1):
                     got.setdefault(k["sa"] + x, []).append((q, "C" if second else "A", o))
