@@ -126,7 +126,7 @@ void Engine::free_all()
     type.release(); atom_struct.release(); atom_cell.release(); grid.release(); bbox.release();
     cell_cnt.release(); cell_start.release(); cell_fill.release(); cell_atoms.release(); scan_tmp.release();
     cell_tcnt.release();
-    cell_pos.release(); order.release(); type_fill.release();
+    cell_pos.release(); order.release(); type_fill.release(); neigh_items.release();
     nbr.release(); nbr_cnt.release(); G.release(); dEdG.release(); e_atom.release();
     e_struct.release(); force.release(); symm_d.release(); err.release(); vir.release(); eatom_d.release();
     tvec.release(); gE.release(); tang.release(); pgrad.release();

@@ -120,7 +120,8 @@ struct Engine {
     DBuf<int> cell_tcnt;          // members of each type per cell [cell][type]
     DBuf<double4> cell_pos;       // cell-ordered wrapped positions, type in .w
     DBuf<int> order;              // atoms grouped by element (visiting order of the per-atom kernels)
-    DBuf<int> type_fill;          // [2 * (NNP_MAX_TYPES + 1)] element counts (out-of-range types last) and fill cursors
+    DBuf<int> type_fill;          // [2 * (NNP_MAX_TYPES + 1) + 1] element counts (out-of-range types last), fill cursors, neighbour-search work items
+    DBuf<int4> neigh_items;       // neighbour-search work items {cell, structure, first atom, end atom}
     DBuf<float4> nbr;
     DBuf<int> nbr_cnt;
     DBuf<float> G, dEdG, e_atom;

@@ -7,8 +7,8 @@
 //   k_bin          wrap atoms into their cell, count atoms per cell
 //   k_cell_start   per-structure scan of the cell counts
 //   k_fill, k_sort_cells   cell member lists, sorted by type and atom index
-//   k_neigh        one block per cell: candidates from the (2m+1)^3 cells
-//                  gathered in shared memory, one warp per atom of the cell,
+//   k_neigh        one block per cell or part of a cell: candidates from the
+//                  (2m+1)^3 cells gathered in shared memory, one warp per atom,
 //                  exact FP64 displacement test, neighbours grouped by type
 //                  (replaces NeighborList::build, struc/neighbor.cpp:46-87)
 //   k_symm         one warp per atom: radial + angular symmetry functions
@@ -302,6 +302,28 @@ __global__ void k_fill(int64_t N, const int *__restrict__ atom_cell, const int *
     cell_atoms[slot] = (int)i;
 }
 
+#define NEIGH_WARPS 4         // warps per block of the neighbour search
+#define NEIGH_THREADS (NEIGH_WARPS * 32)
+#define NEIGH_BLOCKS 7        // resident blocks per SM (shared memory)
+#define NEIGH_CAND 768       // candidates held in shared memory at a time (multiple of 64)
+#define NEIGH_ENT 512         // (type, neighbouring cell) segments of one cell's candidate list
+#define NEIGH_ATOMS 1024      // atoms of one cell whose counts are kept while chunks stream
+#define NEIGH_ITEM_COUNTER (2 * (NNP_MAX_TYPES + 1))   // type_fill entry counting the neighbour-search work items
+
+// Work items of the neighbour search: the atoms of a cell split into parts of
+// about `budget` candidate tests (atoms x candidates, the candidates estimated
+// as the cell's own count times the O = (2m+1)^3 cells searched), one atom
+// per warp at the finest.  A big cell (a small periodic structure is one cell
+// seen through its 27 images) then spreads over several blocks instead of
+// setting the search's time on one.
+__device__ __forceinline__ int neigh_parts(int n, int O, int budget)
+{
+    if (n <= 0) return 0;
+    const int64_t p = ((int64_t)O * n * n + budget - 1) / budget;
+    const int pmax = (n + NEIGH_WARPS - 1) / NEIGH_WARPS;
+    return (int)(p < 1 ? 1 : (p > pmax ? pmax : p));
+}
+
 // Sort key of a cell member: type in the top 4 bits (atom indices < 2^28); a
 // type outside [0, ntypes) gets 15, sorts last and is counted for no type.
 __device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
@@ -311,32 +333,59 @@ __device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
 }
 
 // The members of every cell (all structures) sorted by (type, atom index)
-// and counted per type.  A lane sorts a cell of at most 64 atoms in registers
-// (insertion sort); the warp then ranks its larger cells together, one at a
-// time: the keys type << 28 | atom are distinct, so a key's place is the
-// number of smaller keys (the same order as any comparison sort), each lane
-// ranking four of its keys per load of a compared key.  Those keys sit in the
-// warp's shared memory, or for a cell of more than SORT_SMEM atoms (a free
-// structure of up to NNP_FREE_ONE_CELL atoms is one cell) in tmp at the
-// cell's own slots.
+// and counted per type, and the cell's neighbour-search work items.  A lane
+// sorts a cell of at most SORT_LANE atoms (its keys gathered first, with
+// independent loads, then insertion-sorted); the warp then ranks its larger
+// cells together, one at a time: the keys type << 28 | atom are distinct, so
+// a key's place is the number of smaller keys (the same order as any
+// comparison sort), each lane ranking four of its keys per load of a compared
+// key.  Those keys sit in the warp's shared memory, or for a cell of more
+// than SORT_SMEM atoms (a free structure of up to NNP_FREE_ONE_CELL atoms is
+// one cell) in tmp at the cell's own slots.  Each cell appends its parts
+// (neigh_parts) to `items` as {cell, structure, first atom, end atom}, at a
+// place taken from items_n.
 #define SORT_WARPS 4
 #define SORT_SMEM 512
+#define SORT_LANE 32
 __global__ void __launch_bounds__(SORT_WARPS * 32)
 k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
              const int *__restrict__ cell_cnt, const int *__restrict__ cell_start, const int *__restrict__ type,
-             int ntypes, int *__restrict__ cell_atoms, int *__restrict__ cell_tcnt, unsigned *__restrict__ tmp)
+             const int *__restrict__ atom_struct, int ntypes, int budget, int *__restrict__ cell_atoms,
+             int *__restrict__ cell_tcnt, unsigned *__restrict__ tmp, int4 *__restrict__ items,
+             int *__restrict__ items_n)
 {
     __shared__ unsigned keys[SORT_WARPS][SORT_SMEM];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = c < grid[S - 1].cell_base + ncells[S - 1];
     const int n = valid ? cell_cnt[c] : 0;
-    if (valid && n <= 64) {
+    {
+        int s = 0, parts = 0;
+        if (n > 0) {
+            s = atom_struct[cell_atoms[cell_start[c]]];
+            const StructGrid &g = grid[s];
+            parts = neigh_parts(n, (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1), budget);
+        }
+        int inc = parts;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += u;
+        }
+        int base = 0;
+        if (lane == 31 && inc > 0) base = atomicAdd(items_n, inc);
+        base = __shfl_sync(0xffffffffu, base, 31) + inc - parts;
+        for (int p = 0; p < parts; ++p)
+            items[base + p] = make_int4(c, s, (int)((int64_t)p * n / parts), (int)((int64_t)(p + 1) * n / parts));
+    }
+    if (valid && n <= SORT_LANE) {
         int *a = cell_atoms + cell_start[c];
         int *tc = cell_tcnt + (size_t)c * ntypes;
-        int key[64];
-        for (int p = 0; p < n; ++p) {
-            const unsigned v = sort_key(a[p], type[a[p]], ntypes);
+        int key[SORT_LANE];
+#pragma unroll 4
+        for (int p = 0; p < n; ++p) key[p] = (int)sort_key(a[p], type[a[p]], ntypes);
+        for (int p = 1; p < n; ++p) {
+            const unsigned v = (unsigned)key[p];
             int q = p - 1;
             while (q >= 0 && (unsigned)key[q] > v) { key[q + 1] = key[q]; --q; }
             key[q + 1] = (int)v;
@@ -350,7 +399,7 @@ k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__
         }
         for (; p < n; ++p) a[p] = key[p] & 0x0fffffff;          // out-of-range types, last
     }
-    unsigned big = __ballot_sync(0xffffffffu, valid && n > 64);
+    unsigned big = __ballot_sync(0xffffffffu, valid && n > SORT_LANE);
     while (big) {
         const int src = __ffs(big) - 1;
         big &= big - 1;
@@ -399,8 +448,8 @@ __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const 
                                (t >= 0 && t < ntypes) ? (double)t : -1.0);
 }
 
-// Neighbour search, one thread block per cell.  Every atom of a cell has the
-// same candidates: the members of the (2m+1)^3 cells around it, each with its
+// Neighbour search, one thread block per work item: a cell, or a part of its
+// atoms (k_sort_cells).  Every atom of a cell has the same candidates: the members of the (2m+1)^3 cells around it, each with its
 // lattice image shift.  The block gathers them into shared memory with the
 // shift applied in FP64 (x_j + R q), ordered by neighbour type, then by cell
 // offset, then by atom index (cell member lists are sorted by type and index),
@@ -412,12 +461,6 @@ __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const 
 // buffer stream through it in chunks; a cell with more (type, cell) segments
 // than the segment table holds is searched from global memory, one warp per
 // atom, with the same order and arithmetic.
-#define NEIGH_WARPS 4         // warps per block of the neighbour search
-#define NEIGH_THREADS (NEIGH_WARPS * 32)
-#define NEIGH_BLOCKS 7        // resident blocks per SM (shared memory)
-#define NEIGH_CAND 768       // candidates held in shared memory at a time (multiple of 64)
-#define NEIGH_ENT 512         // (type, neighbouring cell) segments of one cell's candidate list
-#define NEIGH_ATOMS 1024      // atoms of one cell whose counts are kept while chunks stream
 
 struct NeighShared {
     union {
@@ -611,8 +654,8 @@ __device__ void search_atom_global(NeighShared &sh, int warp, int lane, int64_t 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(NEIGH_THREADS, NEIGH_BLOCKS) k_neigh(int S, const int *__restrict__ ncells,
-                                                          const int *__restrict__ atom_struct,
+__global__ void __launch_bounds__(NEIGH_THREADS, NEIGH_BLOCKS) k_neigh(const int4 *__restrict__ items,
+                                                          const int *__restrict__ items_n,
                                                           const StructGrid *__restrict__ grid,
                                                           const double4 *__restrict__ cell_pos,
                                                           const int *__restrict__ cell_cnt,
@@ -625,18 +668,18 @@ __global__ void __launch_bounds__(NEIGH_THREADS, NEIGH_BLOCKS) k_neigh(int S, co
     extern __shared__ __align__(16) unsigned char neigh_smem[];
     NeighShared &sh = *reinterpret_cast<NeighShared *>(neigh_smem);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int total_cells = grid[S - 1].cell_base + ncells[S - 1];
-    for (int c = blockIdx.x; c < total_cells; c += gridDim.x) {
-        const int na = cell_cnt[c];
-        if (na == 0) continue;                                   // uniform over the block
+    const int nitems = *items_n;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {  // uniform over the block
+        const int4 w = items[it];
+        const int c = w.x, a_lo = w.z, a_hi = w.w;
         const int cs = cell_start[c];
-        const StructGrid &g = grid[atom_struct[cell_atoms[cs]]];
+        const StructGrid &g = grid[w.y];
         const int local = c - g.cell_base;
         const int c2 = local % g.nc[2], c1 = (local / g.nc[2]) % g.nc[1], c0 = local / (g.nc[1] * g.nc[2]);
         const int O = (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1);
         const int NE = ntypes * O;
         if (NE > NEIGH_ENT) {
-            for (int a = warp; a < na; a += NEIGH_WARPS) {
+            for (int a = a_lo + warp; a < a_hi; a += NEIGH_WARPS) {
                 const double4 xi = cell_pos[cs + a];
                 search_atom_global(sh, warp, lane, cell_atoms[cs + a], g, c0, c1, c2, xi.x, xi.y, xi.z, cell_pos,
                                    cell_cnt, cell_start, cell_atoms, rc2, cap, ntypes, nbr, nbr_cnt, err);
@@ -679,15 +722,15 @@ __global__ void __launch_bounds__(NEIGH_THREADS, NEIGH_BLOCKS) k_neigh(int S, co
             const int kp = (T + 63) & ~63;
             load_candidates(sh, 0, T, kp, NE, g, cell_pos, cell_atoms, tid);
             __syncthreads();
-            for (int a = warp; a < na; a += NEIGH_WARPS) {
+            for (int a = a_lo + warp; a < a_hi; a += NEIGH_WARPS) {
                 const int i = cell_atoms[cs + a];
                 const double4 xi = cell_pos[cs + a];
                 const int count = test_candidates(sh, kp, lane, i, xi.x, xi.y, xi.z, rc2, 0, cap, nbr + (int64_t)i * cap);
                 if (lane == 0) finish_atom(i, count, cap, nbr_cnt, err);
             }
         } else {
-            for (int a0 = 0; a0 < na; a0 += NEIGH_ATOMS) {
-                const int a1 = min(na, a0 + NEIGH_ATOMS);
+            for (int a0 = a_lo; a0 < a_hi; a0 += NEIGH_ATOMS) {
+                const int a1 = min(a_hi, a0 + NEIGH_ATOMS);
                 for (int a = a0 + tid; a < a1; a += NEIGH_THREADS) sh.count[a - a0] = 0;
                 for (int k0 = 0; k0 < T; k0 += NEIGH_CAND) {
                     const int k1 = min(T, k0 + NEIGH_CAND), kp = (k1 - k0 + 63) & ~63;
@@ -1125,7 +1168,8 @@ std::string run_prepare(Engine &E, int64_t n_atoms, int n_struct, int pbc)
     r(E.cell_atoms.reserve(N));
     r(E.cell_pos.reserve(N));
     r(E.order.reserve(N));
-    r(E.type_fill.reserve(2 * (NNP_MAX_TYPES + 1)));
+    r(E.type_fill.reserve(NEIGH_ITEM_COUNTER + 1));
+    r(E.neigh_items.reserve(N + (N + NEIGH_WARPS - 1) / NEIGH_WARPS + 1));   // parts: at most one per cell and one per warp's atom
     r(E.nbr.reserve(N * (size_t)E.cap));
     r(E.nbr_cnt.reserve(N));
     r(E.G.reserve(N * (size_t)E.gstride));
@@ -1147,7 +1191,7 @@ std::string run_neighbors(Engine &E, int pbc)
     cudaStream_t st = E.stream;
     E.mark(0);
     E.launches += 12;
-    cudaMemsetAsync(E.type_fill.p, 0, 2 * (NNP_MAX_TYPES + 1) * sizeof(int), st);
+    cudaMemsetAsync(E.type_fill.p, 0, (NEIGH_ITEM_COUNTER + 1) * sizeof(int), st);
     k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p);
     k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p,
                                                                E.type_fill.p + NNP_MAX_TYPES + 1, E.order.p);
@@ -1164,16 +1208,21 @@ std::string run_neighbors(Engine &E, int pbc)
                                                      E.cell_cnt.p);
     k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
     k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
+    // candidate tests per work item: about half a block's share of the
+    // search, estimated at 432 tests per atom (27 cells of 16 atoms)
+    const int nblocks = num_sms() * NEIGH_BLOCKS;
+    const int budget = (int)std::min<int64_t>(1 << 16, std::max<int64_t>(2048, N * 216 / nblocks));
+    int *items_n = E.type_fill.p + NEIGH_ITEM_COUNTER;
     // (atom_cell, read only by k_fill, holds the keys of the largest cells)
     k_sort_cells<<<grid_for((int64_t)cell_bound, SORT_WARPS * 32, 1 << 30), SORT_WARPS * 32, 0, st>>>(
-        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.dpot.ntypes, E.cell_atoms.p, E.cell_tcnt.p,
-        reinterpret_cast<unsigned *>(E.atom_cell.p));
+        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.atom_struct.p, E.dpot.ntypes, budget,
+        E.cell_atoms.p, E.cell_tcnt.p, reinterpret_cast<unsigned *>(E.atom_cell.p), E.neigh_items.p, items_n);
     k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
                                                           E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     const int nsm = sizeof(NeighShared);
     cudaFuncSetAttribute(k_neigh, cudaFuncAttributeMaxDynamicSharedMemorySize, nsm);
-    k_neigh<<<num_sms() * NEIGH_BLOCKS, NEIGH_THREADS, nsm, st>>>(S, E.scan_tmp.p, E.atom_struct.p, E.grid.p, E.cell_pos.p,
+    k_neigh<<<nblocks, NEIGH_THREADS, nsm, st>>>(E.neigh_items.p, items_n, E.grid.p, E.cell_pos.p,
                                                        E.cell_cnt.p, E.cell_start.p, E.cell_tcnt.p, E.cell_atoms.p,
                                                        rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
     E.mark(1);
