@@ -333,20 +333,18 @@ __device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
 }
 
 // The members of every cell (all structures) sorted by (type, atom index)
-// and counted per type, and the cell's neighbour-search work items.  A lane
-// sorts a cell of at most SORT_LANE atoms (its keys gathered first, with
-// independent loads, then insertion-sorted); the warp then ranks its larger
-// cells together, one at a time: the keys type << 28 | atom are distinct, so
-// a key's place is the number of smaller keys (the same order as any
-// comparison sort), each lane ranking four of its keys per load of a compared
-// key.  Those keys sit in the warp's shared memory, or for a cell of more
-// than SORT_SMEM atoms (a free structure of up to NNP_FREE_ONE_CELL atoms is
-// one cell) in tmp at the cell's own slots.  Each cell appends its parts
+// and counted per type, and the cell's neighbour-search work items; one warp
+// per cell, the warps striding over all cells.  The keys type << 28 | atom
+// are distinct, so a key's place is the number of smaller keys (the same
+// order as any comparison sort): a cell of at most 32 atoms has one key per
+// lane, a larger one is ranked four keys per lane per load of a compared key.
+// The keys sit in the warp's shared memory, or for a cell of more than
+// SORT_SMEM atoms (a free structure of up to NNP_FREE_ONE_CELL atoms is one
+// cell) in tmp at the cell's own slots.  Each cell appends its parts
 // (neigh_parts) to `items` as {cell, structure, first atom, end atom}, at a
 // place taken from items_n.
 #define SORT_WARPS 4
 #define SORT_SMEM 512
-#define SORT_LANE 32
 __global__ void __launch_bounds__(SORT_WARPS * 32)
 k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
              const int *__restrict__ cell_cnt, const int *__restrict__ cell_start, const int *__restrict__ type,
@@ -356,82 +354,63 @@ k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__
 {
     __shared__ unsigned keys[SORT_WARPS][SORT_SMEM];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = c < grid[S - 1].cell_base + ncells[S - 1];
-    const int n = valid ? cell_cnt[c] : 0;
-    {
-        int s = 0, parts = 0;
-        if (n > 0) {
-            s = atom_struct[cell_atoms[cell_start[c]]];
+    const int total = grid[S - 1].cell_base + ncells[S - 1];
+    for (int c = blockIdx.x * SORT_WARPS + warp; c < total; c += gridDim.x * SORT_WARPS) {
+        const int n = cell_cnt[c];
+        if (n == 0) continue;                                    // uniform over the warp
+        const int cs = cell_start[c];
+        int *a = cell_atoms + cs;
+        unsigned *k = (n <= SORT_SMEM) ? keys[warp] : tmp + cs;
+        for (int p = lane; p < n; p += 32) k[p] = sort_key(a[p], type[a[p]], ntypes);
+        int s = 0, parts = 0, base = 0;
+        if (lane == 0) {
+            s = atom_struct[a[0]];
             const StructGrid &g = grid[s];
             parts = neigh_parts(n, (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1), budget);
+            base = atomicAdd(items_n, parts);
         }
-        int inc = parts;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, inc, d);
-            if (lane >= d) inc += u;
-        }
-        int base = 0;
-        if (lane == 31 && inc > 0) base = atomicAdd(items_n, inc);
-        base = __shfl_sync(0xffffffffu, base, 31) + inc - parts;
-        for (int p = 0; p < parts; ++p)
+        s = __shfl_sync(0xffffffffu, s, 0);
+        parts = __shfl_sync(0xffffffffu, parts, 0);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        for (int p = lane; p < parts; p += 32)
             items[base + p] = make_int4(c, s, (int)((int64_t)p * n / parts), (int)((int64_t)(p + 1) * n / parts));
-    }
-    if (valid && n <= SORT_LANE) {
-        int *a = cell_atoms + cell_start[c];
-        int *tc = cell_tcnt + (size_t)c * ntypes;
-        int key[SORT_LANE];
-#pragma unroll 4
-        for (int p = 0; p < n; ++p) key[p] = (int)sort_key(a[p], type[a[p]], ntypes);
-        for (int p = 1; p < n; ++p) {
-            const unsigned v = (unsigned)key[p];
-            int q = p - 1;
-            while (q >= 0 && (unsigned)key[q] > v) { key[q + 1] = key[q]; --q; }
-            key[q + 1] = (int)v;
-        }
-        int p = 0;
-        for (int t = 0; t < ntypes; ++t) {
-            int q = p;
-            while (q < n && ((unsigned)key[q] >> 28) == (unsigned)t) { a[q] = key[q] & 0x0fffffff; ++q; }
-            tc[t] = q - p;
-            p = q;
-        }
-        for (; p < n; ++p) a[p] = key[p] & 0x0fffffff;          // out-of-range types, last
-    }
-    unsigned big = __ballot_sync(0xffffffffu, valid && n > SORT_LANE);
-    while (big) {
-        const int src = __ffs(big) - 1;
-        big &= big - 1;
-        const int cc = __shfl_sync(0xffffffffu, c, src), nn = __shfl_sync(0xffffffffu, n, src);
-        int *a = cell_atoms + cell_start[cc];
-        unsigned *k = (nn <= SORT_SMEM) ? keys[warp] : tmp + cell_start[cc];
-        for (int p = lane; p < nn; p += 32) k[p] = sort_key(a[p], type[a[p]], ntypes);
         __threadfence_block();
-        __syncwarp();
-        for (int p0 = lane; p0 < nn; p0 += 128) {
-            unsigned v[4];
-            int r[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                v[u] = (p0 + 32 * u < nn) ? k[p0 + 32 * u] : 0xffffffffu;
-                r[u] = 0;
+        __syncwarp();                                            // keys written, a[0] read
+        int *tc = cell_tcnt + (size_t)c * ntypes;
+        if (n <= 32) {
+            const unsigned v = lane < n ? k[lane] : 0xffffffffu;
+            int r = 0;
+            for (int q = 0; q < n; ++q) r += (k[q] < v) ? 1 : 0;
+            if (lane < n) a[r] = (int)(v & 0x0fffffffu);
+            for (int t = 0; t < ntypes; ++t) {
+                const int m = __popc(__ballot_sync(0xffffffffu, lane < n && (v >> 28) == (unsigned)t));
+                if (lane == 0) tc[t] = m;
             }
-            for (int q = 0; q < nn; ++q) {
-                const unsigned w = k[q];
+        } else {
+            for (int p0 = lane; p0 < n; p0 += 128) {
+                unsigned v[4];
+                int r[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) r[u] += (w < v[u]) ? 1 : 0;
+                for (int u = 0; u < 4; ++u) {
+                    v[u] = (p0 + 32 * u < n) ? k[p0 + 32 * u] : 0xffffffffu;
+                    r[u] = 0;
+                }
+                for (int q = 0; q < n; ++q) {
+                    const unsigned w = k[q];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) r[u] += (w < v[u]) ? 1 : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (p0 + 32 * u < n) a[r[u]] = (int)(v[u] & 0x0fffffffu);
             }
+            for (int t = 0; t < ntypes; ++t) {
+                int m = 0;
+                for (int p = lane; p < n; p += 32) m += ((k[p] >> 28) == (unsigned)t) ? 1 : 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (p0 + 32 * u < nn) a[r[u]] = (int)(v[u] & 0x0fffffffu);
-        }
-        for (int t = 0; t < ntypes; ++t) {
-            int m = 0;
-            for (int p = lane; p < nn; p += 32) m += ((k[p] >> 28) == (unsigned)t) ? 1 : 0;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
-            if (lane == 0) cell_tcnt[(size_t)cc * ntypes + t] = m;
+                for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+                if (lane == 0) tc[t] = m;
+            }
         }
         __syncwarp();                                            // keys[warp] reused by the next cell
     }
@@ -1214,7 +1193,7 @@ std::string run_neighbors(Engine &E, int pbc)
     const int budget = (int)std::min<int64_t>(1 << 16, std::max<int64_t>(2048, N * 216 / nblocks));
     int *items_n = E.type_fill.p + NEIGH_ITEM_COUNTER;
     // (atom_cell, read only by k_fill, holds the keys of the largest cells)
-    k_sort_cells<<<grid_for((int64_t)cell_bound, SORT_WARPS * 32, 1 << 30), SORT_WARPS * 32, 0, st>>>(
+    k_sort_cells<<<num_sms() * 16, SORT_WARPS * 32, 0, st>>>(
         S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.atom_struct.p, E.dpot.ntypes, budget,
         E.cell_atoms.p, E.cell_tcnt.p, reinterpret_cast<unsigned *>(E.atom_cell.p), E.neigh_items.p, items_n);
     k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
