@@ -50,11 +50,10 @@ static std::string cuda_msg(const char *what)
 
 // ------------------------------------------------------------------ structure grids
 
-__global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N, int *__restrict__ atom_struct,
-                              const int *__restrict__ type, int ntypes, DevErr *err)
+__device__ __forceinline__ void atom_struct_one(int64_t i, const int64_t *__restrict__ off, int S,
+                                                int *__restrict__ atom_struct, const int *__restrict__ type,
+                                                int ntypes, DevErr *err)
 {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
     int lo = 0, hi = S - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -64,6 +63,13 @@ __global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N,
     atom_struct[i] = lo;
     const int t = type[i];
     if (t < 0 || t >= ntypes) atomicMax(&err->bad_type, 1);
+}
+
+__global__ void k_atom_struct(const int64_t *__restrict__ off, int S, int64_t N, int *__restrict__ atom_struct,
+                              const int *__restrict__ type, int ntypes, DevErr *err)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < N) atom_struct_one(i, off, S, atom_struct, type, ntypes, err);
 }
 
 // Atoms grouped by element: per-block counts in shared memory, one global
@@ -143,12 +149,10 @@ __global__ void k_struct_bbox(const double *__restrict__ pos, const int64_t *__r
 // candidate of every other).
 #define NNP_FREE_ONE_CELL 2048
 
-__global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *__restrict__ off, int S, int pbc,
-                               double rc, const double *__restrict__ bbox, StructGrid *__restrict__ grid,
-                               int *__restrict__ ncells, DevErr *err)
+__device__ void struct_setup_one(int s, const double *__restrict__ cell, const int64_t *__restrict__ off, int pbc,
+                                 double rc, const double *__restrict__ bbox, StructGrid *__restrict__ grid,
+                                 int *__restrict__ ncells, DevErr *err)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S) return;
     StructGrid g;
     const int64_t nat = off[s + 1] - off[s];
     for (int k = 0; k < 9; ++k) { g.R[k] = 0.0; g.B[k] = 0.0; }
@@ -207,6 +211,14 @@ __global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *_
     ncells[s] = g.nc[0] * g.nc[1] * g.nc[2];
 }
 
+__global__ void k_struct_setup(const double *__restrict__ cell, const int64_t *__restrict__ off, int S, int pbc,
+                               double rc, const double *__restrict__ bbox, StructGrid *__restrict__ grid,
+                               int *__restrict__ ncells, DevErr *err)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) struct_setup_one(s, cell, off, pbc, rc, bbox, grid, ncells, err);
+}
+
 // exclusive scan of ncells over structures in one block; writes cell_base
 __global__ void k_cell_base(const int *__restrict__ ncells, int S, StructGrid *__restrict__ grid)
 {
@@ -231,12 +243,10 @@ __global__ void k_cell_base(const int *__restrict__ ncells, int S, StructGrid *_
     }
 }
 
-__global__ void k_bin(int64_t N, const double *__restrict__ pos, const int *__restrict__ atom_struct,
-                      const StructGrid *__restrict__ grid, double *__restrict__ xw, int *__restrict__ atom_cell,
-                      int *__restrict__ cell_cnt)
+__device__ __forceinline__ void bin_one(int64_t i, const double *__restrict__ pos, const int *__restrict__ atom_struct,
+                                        const StructGrid *__restrict__ grid, double *__restrict__ xw,
+                                        int *__restrict__ atom_cell, int *__restrict__ cell_cnt)
 {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
     const StructGrid &g = grid[atom_struct[i]];
     const double x[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
     int cid = g.cell_base;
@@ -262,6 +272,14 @@ __global__ void k_bin(int64_t N, const double *__restrict__ pos, const int *__re
     xw[3 * i + 2] = y[2];
     atom_cell[i] = cid;
     atomicAdd(&cell_cnt[cid], 1);
+}
+
+__global__ void k_bin(int64_t N, const double *__restrict__ pos, const int *__restrict__ atom_struct,
+                      const StructGrid *__restrict__ grid, double *__restrict__ xw, int *__restrict__ atom_cell,
+                      int *__restrict__ cell_cnt)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < N) bin_one(i, pos, atom_struct, grid, xw, atom_cell, cell_cnt);
 }
 
 // one block per structure: exclusive scan of its cells' counts
@@ -345,6 +363,72 @@ __device__ __forceinline__ unsigned sort_key(int atom, int t, int ntypes)
 // place taken from items_n.
 #define SORT_WARPS 4
 #define SORT_SMEM 512
+// one cell by one warp; keys: the warp's shared buffer of kcap entries
+__device__ void sort_cell(int c, int lane, unsigned *keys, int kcap, const StructGrid *__restrict__ grid,
+                          const int *__restrict__ cell_cnt, const int *__restrict__ cell_start,
+                          const int *__restrict__ type, const int *__restrict__ atom_struct, int ntypes, int budget,
+                          int *__restrict__ cell_atoms, int *__restrict__ cell_tcnt, unsigned *__restrict__ tmp,
+                          int4 *__restrict__ items, int *__restrict__ items_n)
+{
+    const int n = cell_cnt[c];
+    if (n == 0) return;                                          // uniform over the warp
+    const int cs = cell_start[c];
+    int *a = cell_atoms + cs;
+    unsigned *k = (n <= kcap) ? keys : tmp + cs;
+    for (int p = lane; p < n; p += 32) k[p] = sort_key(a[p], type[a[p]], ntypes);
+    int s = 0, parts = 0, base = 0;
+    if (lane == 0) {
+        s = atom_struct[a[0]];
+        const StructGrid &g = grid[s];
+        parts = neigh_parts(n, (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1), budget);
+        base = atomicAdd(items_n, parts);
+    }
+    s = __shfl_sync(0xffffffffu, s, 0);
+    parts = __shfl_sync(0xffffffffu, parts, 0);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int p = lane; p < parts; p += 32)
+        items[base + p] = make_int4(c, s, (int)((int64_t)p * n / parts), (int)((int64_t)(p + 1) * n / parts));
+    __threadfence_block();
+    __syncwarp();                                                // keys written, a[0] read
+    int *tc = cell_tcnt + (size_t)c * ntypes;
+    if (n <= 32) {
+        const unsigned v = lane < n ? k[lane] : 0xffffffffu;
+        int r = 0;
+        for (int q = 0; q < n; ++q) r += (k[q] < v) ? 1 : 0;
+        if (lane < n) a[r] = (int)(v & 0x0fffffffu);
+        for (int t = 0; t < ntypes; ++t) {
+            const int m = __popc(__ballot_sync(0xffffffffu, lane < n && (v >> 28) == (unsigned)t));
+            if (lane == 0) tc[t] = m;
+        }
+    } else {
+        for (int p0 = lane; p0 < n; p0 += 128) {
+            unsigned v[4];
+            int r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] = (p0 + 32 * u < n) ? k[p0 + 32 * u] : 0xffffffffu;
+                r[u] = 0;
+            }
+            for (int q = 0; q < n; ++q) {
+                const unsigned w = k[q];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) r[u] += (w < v[u]) ? 1 : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (p0 + 32 * u < n) a[r[u]] = (int)(v[u] & 0x0fffffffu);
+        }
+        for (int t = 0; t < ntypes; ++t) {
+            int m = 0;
+            for (int p = lane; p < n; p += 32) m += ((k[p] >> 28) == (unsigned)t) ? 1 : 0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+            if (lane == 0) tc[t] = m;
+        }
+    }
+    __syncwarp();                                                // keys reused by the next cell
+}
+
 __global__ void __launch_bounds__(SORT_WARPS * 32)
 k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__ ncells,
              const int *__restrict__ cell_cnt, const int *__restrict__ cell_start, const int *__restrict__ type,
@@ -355,76 +439,122 @@ k_sort_cells(int S, const StructGrid *__restrict__ grid, const int *__restrict__
     __shared__ unsigned keys[SORT_WARPS][SORT_SMEM];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = grid[S - 1].cell_base + ncells[S - 1];
-    for (int c = blockIdx.x * SORT_WARPS + warp; c < total; c += gridDim.x * SORT_WARPS) {
-        const int n = cell_cnt[c];
-        if (n == 0) continue;                                    // uniform over the warp
-        const int cs = cell_start[c];
-        int *a = cell_atoms + cs;
-        unsigned *k = (n <= SORT_SMEM) ? keys[warp] : tmp + cs;
-        for (int p = lane; p < n; p += 32) k[p] = sort_key(a[p], type[a[p]], ntypes);
-        int s = 0, parts = 0, base = 0;
-        if (lane == 0) {
-            s = atom_struct[a[0]];
-            const StructGrid &g = grid[s];
-            parts = neigh_parts(n, (2 * g.m[0] + 1) * (2 * g.m[1] + 1) * (2 * g.m[2] + 1), budget);
-            base = atomicAdd(items_n, parts);
-        }
-        s = __shfl_sync(0xffffffffu, s, 0);
-        parts = __shfl_sync(0xffffffffu, parts, 0);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        for (int p = lane; p < parts; p += 32)
-            items[base + p] = make_int4(c, s, (int)((int64_t)p * n / parts), (int)((int64_t)(p + 1) * n / parts));
-        __threadfence_block();
-        __syncwarp();                                            // keys written, a[0] read
-        int *tc = cell_tcnt + (size_t)c * ntypes;
-        if (n <= 32) {
-            const unsigned v = lane < n ? k[lane] : 0xffffffffu;
-            int r = 0;
-            for (int q = 0; q < n; ++q) r += (k[q] < v) ? 1 : 0;
-            if (lane < n) a[r] = (int)(v & 0x0fffffffu);
-            for (int t = 0; t < ntypes; ++t) {
-                const int m = __popc(__ballot_sync(0xffffffffu, lane < n && (v >> 28) == (unsigned)t));
-                if (lane == 0) tc[t] = m;
-            }
-        } else {
-            for (int p0 = lane; p0 < n; p0 += 128) {
-                unsigned v[4];
-                int r[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    v[u] = (p0 + 32 * u < n) ? k[p0 + 32 * u] : 0xffffffffu;
-                    r[u] = 0;
-                }
-                for (int q = 0; q < n; ++q) {
-                    const unsigned w = k[q];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) r[u] += (w < v[u]) ? 1 : 0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (p0 + 32 * u < n) a[r[u]] = (int)(v[u] & 0x0fffffffu);
-            }
-            for (int t = 0; t < ntypes; ++t) {
-                int m = 0;
-                for (int p = lane; p < n; p += 32) m += ((k[p] >> 28) == (unsigned)t) ? 1 : 0;
-#pragma unroll
-                for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
-                if (lane == 0) tc[t] = m;
-            }
-        }
-        __syncwarp();                                            // keys[warp] reused by the next cell
-    }
+    for (int c = blockIdx.x * SORT_WARPS + warp; c < total; c += gridDim.x * SORT_WARPS)
+        sort_cell(c, lane, keys[warp], SORT_SMEM, grid, cell_cnt, cell_start, type, atom_struct, ntypes, budget,
+                  cell_atoms, cell_tcnt, tmp, items, items_n);
+}
+
+__device__ __forceinline__ void cell_pos_one(int64_t s, const int *__restrict__ cell_atoms,
+                                             const double *__restrict__ xw, const int *__restrict__ type, int ntypes,
+                                             double4 *__restrict__ cell_pos)
+{
+    const int a = cell_atoms[s];
+    const int t = type[a];
+    cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2],
+                               (t >= 0 && t < ntypes) ? (double)t : -1.0);
 }
 
 __global__ void k_cell_pos(int64_t N, const int *__restrict__ cell_atoms, const double *__restrict__ xw,
                            const int *__restrict__ type, int ntypes, double4 *__restrict__ cell_pos)
 {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s >= N) return;
-    const int a = cell_atoms[s];
-    const int t = type[a];
-    cell_pos[s] = make_double4(xw[3 * (int64_t)a], xw[3 * (int64_t)a + 1], xw[3 * (int64_t)a + 2],
-                               (t >= 0 && t < ntypes) ? (double)t : -1.0);
+    if (s < N) cell_pos_one(s, cell_atoms, xw, type, ntypes, cell_pos);
+}
+
+// The neighbour-search prologue of a small periodic batch (one MD-style cell
+// or a few) in one thread block: the steps of the launch sequence k_type_count
+// ... k_cell_pos with block barriers between them instead of launches, on the
+// same device functions.  Element counts and fill cursors land in type_fill
+// as k_type_count / k_type_scatter leave them; `order` lists each element's
+// atoms in some order (every consumer treats atoms independently); cell
+// starts are one warp's scan per structure.
+#define PRO_THREADS 1024
+#define PRO_MAX_ATOMS 2048
+#define PRO_MAX_STRUCT 32
+#define PRO_SORT_SMEM 256
+__global__ void __launch_bounds__(PRO_THREADS)
+k_prologue_small(int64_t N, int64_t n_centre, int S, int cell_bound, const int64_t *__restrict__ off,
+                 const double *__restrict__ pos, const double *__restrict__ cell, const int *__restrict__ type,
+                 int ntypes, double rc, int budget, StructGrid *__restrict__ grid, int *__restrict__ ncells,
+                 int *__restrict__ atom_struct, double *__restrict__ xw, int *__restrict__ atom_cell,
+                 int *__restrict__ cell_cnt, int *__restrict__ cell_start, int *__restrict__ cell_fill,
+                 int *__restrict__ cell_atoms, int *__restrict__ cell_tcnt, double4 *__restrict__ cell_pos,
+                 int *__restrict__ type_fill, int *__restrict__ order, int4 *__restrict__ items, DevErr *err)
+{
+    __shared__ int cnt[NNP_MAX_TYPES + 1], cur[NNP_MAX_TYPES + 1], tbase[NNP_MAX_TYPES + 1];
+    __shared__ unsigned keys[PRO_THREADS / 32][PRO_SORT_SMEM];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    int *items_n = type_fill + NEIGH_ITEM_COUNTER;
+    if (t <= NNP_MAX_TYPES) {
+        cnt[t] = 0;
+        cur[t] = 0;
+    }
+    if (t == 0) *items_n = 0;
+    for (int c = t; c < cell_bound; c += PRO_THREADS) cell_cnt[c] = 0;
+    __syncthreads();
+    // atom -> structure, element counts (ghosts and bad types in slot ntypes), structure grids
+    for (int64_t i = t; i < N; i += PRO_THREADS) {
+        atom_struct_one(i, off, S, atom_struct, type, ntypes, err);
+        const int ty = type[i];
+        atomicAdd(&cnt[(ty >= 0 && ty < ntypes && i < n_centre) ? ty : ntypes], 1);
+    }
+    for (int s = t; s < S; s += PRO_THREADS) struct_setup_one(s, cell, off, 1, rc, nullptr, grid, ncells, err);
+    __syncthreads();
+    if (t <= NNP_MAX_TYPES) {
+        int b = 0;
+        for (int k = 0; k < t && k <= ntypes; ++k) b += cnt[k];
+        tbase[t] = b;
+        type_fill[t] = (t <= ntypes) ? cnt[t] : 0;
+        type_fill[NNP_MAX_TYPES + 1 + t] = (t <= ntypes) ? cnt[t] : 0;
+    }
+    if (t == 0) {
+        int run = 0;
+        for (int s = 0; s < S; ++s) {
+            grid[s].cell_base = run;
+            run += ncells[s];
+        }
+    }
+    __syncthreads();
+    // visiting order by element; wrapped positions, cell of each atom, counts
+    for (int64_t i = t; i < N; i += PRO_THREADS) {
+        int ty = type[i];
+        if (!(ty >= 0 && ty < ntypes) || i >= n_centre) ty = ntypes;
+        order[tbase[ty] + atomicAdd(&cur[ty], 1)] = (int)i;
+        bin_one(i, pos, atom_struct, grid, xw, atom_cell, cell_cnt);
+    }
+    __syncthreads();
+    for (int s = warp; s < S; s += PRO_THREADS / 32) {
+        const int base = grid[s].cell_base, nc = ncells[s];
+        int run = (int)off[s];
+        for (int c0 = 0; c0 < nc; c0 += 32) {
+            const int c = c0 + lane;
+            const int v = c < nc ? cell_cnt[base + c] : 0;
+            int inc = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc += u;
+            }
+            if (c < nc) {
+                cell_start[base + c] = run + inc - v;
+                cell_fill[base + c] = 0;
+            }
+            run += __shfl_sync(0xffffffffu, inc, 31);
+        }
+    }
+    __syncthreads();
+    for (int64_t i = t; i < N; i += PRO_THREADS) {
+        const int c = atom_cell[i];
+        cell_atoms[cell_start[c] + atomicAdd(&cell_fill[c], 1)] = (int)i;
+    }
+    __syncthreads();
+    // (atom_cell, read above, holds the keys of cells larger than the shared buffer)
+    const int total = grid[S - 1].cell_base + ncells[S - 1];
+    for (int c = warp; c < total; c += PRO_THREADS / 32)
+        sort_cell(c, lane, keys[warp], PRO_SORT_SMEM, grid, cell_cnt, cell_start, type, atom_struct, ntypes, budget,
+                  cell_atoms, cell_tcnt, reinterpret_cast<unsigned *>(atom_cell), items, items_n);
+    __syncthreads();
+    for (int64_t k = t; k < N; k += PRO_THREADS) cell_pos_one(k, cell_atoms, xw, type, ntypes, cell_pos);
 }
 
 // Neighbour search, one thread block per work item: a cell, or a part of its
@@ -1169,38 +1299,48 @@ std::string run_neighbors(Engine &E, int pbc)
     if (N == 0 || S == 0) return "";
     cudaStream_t st = E.stream;
     E.mark(0);
-    E.launches += 12;
-    cudaMemsetAsync(E.type_fill.p, 0, (NEIGH_ITEM_COUNTER + 1) * sizeof(int), st);
-    k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p);
-    k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p,
-                                                               E.type_fill.p + NNP_MAX_TYPES + 1, E.order.p);
-    k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
-                                                             E.dpot.ntypes, E.err.p);
-    if (!pbc) k_struct_bbox<<<S, 256, 0, st>>>(E.pos.p, E.atom_off.p, E.bbox.p);
-    k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
-                                                              E.bbox.p, E.grid.p, E.scan_tmp.p, E.err.p);
-    E.launches += pbc ? 0 : 1;
-    k_cell_base<<<1, 1024, 0, st>>>(E.scan_tmp.p, S, E.grid.p);
     const size_t cell_bound = 64 * (size_t)S + 2 * (size_t)N + 64;
-    cudaMemsetAsync(E.cell_cnt.p, 0, cell_bound * sizeof(int), st);
-    k_bin<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.pos.p, E.atom_struct.p, E.grid.p, E.xw.p, E.atom_cell.p,
-                                                     E.cell_cnt.p);
-    k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
-    k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
     // candidate tests per work item: about half a block's share of the
     // search, estimated at 432 tests per atom (27 cells of 16 atoms)
     const int nblocks = num_sms() * NEIGH_BLOCKS;
     const int budget = (int)std::min<int64_t>(1 << 16, std::max<int64_t>(2048, N * 216 / nblocks));
     int *items_n = E.type_fill.p + NEIGH_ITEM_COUNTER;
-    // (atom_cell, read only by k_fill, holds the keys of the largest cells)
-    k_sort_cells<<<num_sms() * 16, SORT_WARPS * 32, 0, st>>>(
-        S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.atom_struct.p, E.dpot.ntypes, budget,
-        E.cell_atoms.p, E.cell_tcnt.p, reinterpret_cast<unsigned *>(E.atom_cell.p), E.neigh_items.p, items_n);
-    k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
-                                                          E.cell_pos.p);
     const double rc2 = E.dpot.rc_d * E.dpot.rc_d;
     const int nsm = sizeof(NeighShared);
     cudaFuncSetAttribute(k_neigh, cudaFuncAttributeMaxDynamicSharedMemorySize, nsm);
+    if (pbc && N <= PRO_MAX_ATOMS && S <= PRO_MAX_STRUCT) {
+        // a small periodic batch: the whole prologue in one block
+        E.launches += 2;
+        k_prologue_small<<<1, PRO_THREADS, 0, st>>>(
+            N, E.n_centre, S, (int)cell_bound, E.atom_off.p, E.pos.p, E.cell.p, E.type.p, E.dpot.ntypes,
+            E.dpot.rc_d, budget, E.grid.p, E.scan_tmp.p, E.atom_struct.p, E.xw.p, E.atom_cell.p, E.cell_cnt.p,
+            E.cell_start.p, E.cell_fill.p, E.cell_atoms.p, E.cell_tcnt.p, E.cell_pos.p, E.type_fill.p, E.order.p,
+            E.neigh_items.p, E.err.p);
+    } else {
+        E.launches += 11;
+        cudaMemsetAsync(E.type_fill.p, 0, (NEIGH_ITEM_COUNTER + 1) * sizeof(int), st);
+        k_type_count<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p);
+        k_type_scatter<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.n_centre, E.type.p, E.dpot.ntypes, E.type_fill.p,
+                                                                   E.type_fill.p + NNP_MAX_TYPES + 1, E.order.p);
+        k_atom_struct<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(E.atom_off.p, S, N, E.atom_struct.p, E.type.p,
+                                                                 E.dpot.ntypes, E.err.p);
+        if (!pbc) k_struct_bbox<<<S, 256, 0, st>>>(E.pos.p, E.atom_off.p, E.bbox.p);
+        k_struct_setup<<<grid_for(S, 128, 1 << 30), 128, 0, st>>>(E.cell.p, E.atom_off.p, S, pbc, E.dpot.rc_d,
+                                                                  E.bbox.p, E.grid.p, E.scan_tmp.p, E.err.p);
+        E.launches += pbc ? 0 : 1;
+        k_cell_base<<<1, 1024, 0, st>>>(E.scan_tmp.p, S, E.grid.p);
+        cudaMemsetAsync(E.cell_cnt.p, 0, cell_bound * sizeof(int), st);
+        k_bin<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.pos.p, E.atom_struct.p, E.grid.p, E.xw.p, E.atom_cell.p,
+                                                         E.cell_cnt.p);
+        k_cell_start<<<S, 256, 0, st>>>(E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.cell_fill.p, E.atom_off.p);
+        k_fill<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.atom_cell.p, E.cell_start.p, E.cell_fill.p, E.cell_atoms.p);
+        // (atom_cell, read only by k_fill, holds the keys of the largest cells)
+        k_sort_cells<<<num_sms() * 16, SORT_WARPS * 32, 0, st>>>(
+            S, E.grid.p, E.scan_tmp.p, E.cell_cnt.p, E.cell_start.p, E.type.p, E.atom_struct.p, E.dpot.ntypes, budget,
+            E.cell_atoms.p, E.cell_tcnt.p, reinterpret_cast<unsigned *>(E.atom_cell.p), E.neigh_items.p, items_n);
+        k_cell_pos<<<grid_for(N, 256, 1 << 30), 256, 0, st>>>(N, E.cell_atoms.p, E.xw.p, E.type.p, E.dpot.ntypes,
+                                                              E.cell_pos.p);
+    }
     k_neigh<<<nblocks, NEIGH_THREADS, nsm, st>>>(E.neigh_items.p, items_n, E.grid.p, E.cell_pos.p,
                                                        E.cell_cnt.p, E.cell_start.p, E.cell_tcnt.p, E.cell_atoms.p,
                                                        rc2, E.cap, E.dpot.ntypes, E.nbr.p, E.nbr_cnt.p, E.err.p);
