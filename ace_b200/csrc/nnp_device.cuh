@@ -1071,7 +1071,54 @@ struct GenericBlocks {
     __device__ static bool tangent(const NbrView &, int, int, const Blk &, int, int, float *) { return false; }
     // radial term of one neighbour in the force kernel
     __device__ static bool radial_force(int, int, float, float, float, const float *, float &) { return false; }
+    // one lane's radial sum in the symmetry-function kernel (radial_sum)
+    template <typename Acc>
+    __device__ static bool radial_symm(int, const NbrView &, const float *, float, float, int, int, int, Acc &)
+    {
+        return false;
+    }
+    // one lane's radial tangent sum in the training tangent kernel (radial_tangent_sum)
+    __device__ static bool radial_tangent(int, const NbrView &, const float *, const float *, const float *, float,
+                                          float, int, int, int, float &)
+    {
+        return false;
+    }
 };
+
+// Radial function (rs, eta) of a block whose form is known at compile time,
+// summed over neighbour slots k0, k0 + G, ... < s1 (fcv: the block's cutoff
+// values): the generic loop with the form switch resolved outside it.  Each
+// term is rounded before it is added (no multiply-add contraction across
+// the two), as in the generic loop, so both give the same sums bit for bit.
+__device__ __forceinline__ void acc_term(float &acc, float v) { acc = __fadd_rn(acc, v); }
+__device__ __forceinline__ void acc_term(double &acc, float v) { acc += (double)v; }
+// The tangent kernel's sum of G'(r) rr over the same slots (fdv: cutoff
+// slopes, rr: rates of change of the distances), form fixed at compile time.
+template <int FORM>
+__device__ __forceinline__ float radial_tangent_sum(const NbrView &v, const float *fcv, const float *fdv,
+                                                   const float *rr, float rs, float eta, int k0, int s1, int G)
+{
+    float acc = 0.f;
+    for (int k = k0; k < s1; k += G) {
+        float val, der;
+        radial_fd(FORM, v.r[k], rs, eta, fcv[k], fdv[k], val, der);
+        acc = fmaf(der, rr[k], acc);
+    }
+    return acc;
+}
+
+template <int FORM, typename Acc>
+__device__ __forceinline__ Acc radial_sum(const NbrView &v, const float *fcv, float rs, float eta, int k0, int s1,
+                                          int G)
+{
+    Acc acc = 0;
+    for (int k = k0; k < s1; k += G) {
+        float val, der;
+        radial_fd(FORM, v.r[k], rs, eta, fcv[k], 0.f, val, der);
+        acc_term(acc, val);
+    }
+    return acc;
+}
 
 // ---------------------------------------------------------------- kernel bodies
 
@@ -1109,11 +1156,12 @@ __device__ void symm_body(i64 N, const DevPot *__restrict__ pot, const float2 *_
             Acc acc = 0;
             if (f < B.n) {
                 const float2 q = rpar[B.par + f];
-                for (int k = s0 + ph; k < s1; k += G) {
-                    float val, der;
-                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
-                    acc_add(acc, val, 1.f);
-                }
+                if (!Blocks::template radial_symm<Acc>(B.form, v, v.fc + B.cut * cap, q.x, q.y, s0 + ph, s1, G, acc))
+                    for (int k = s0 + ph; k < s1; k += G) {
+                        float val, der;
+                        radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
+                        acc_add(acc, val, 1.f);
+                    }
             }
             for (int off = 1; off < G; off <<= 1) acc += __shfl_xor_sync(NNP_FULL, acc, off);
             if (ph == 0 && f < B.n) Gi[B.off_g + f] = (float)acc;
@@ -1354,11 +1402,13 @@ __device__ void tangent_body(i64 N, const DevPot *__restrict__ pot, const float2
             float acc = 0.f;
             if (f < B.n) {
                 const float2 q = rpar[B.par + f];
-                for (int k = s0 + ph; k < s1; k += G) {
-                    float val, der;
-                    radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
-                    acc = fmaf(der, rr[k], acc);
-                }
+                if (!Blocks::radial_tangent(B.form, v, v.fc + B.cut * cap, v.fd + B.cut * cap, rr, q.x, q.y, s0 + ph, s1,
+                                            G, acc))
+                    for (int k = s0 + ph; k < s1; k += G) {
+                        float val, der;
+                        radial_fd(B.form, v.r[k], q.x, q.y, v.fc[B.cut * cap + k], v.fd[B.cut * cap + k], val, der);
+                        acc = fmaf(der, rr[k], acc);
+                    }
             }
             for (int off = 1; off < G; off <<= 1) acc += __shfl_xor_sync(NNP_FULL, acc, off);
             if (ph == 0 && f < B.n) Ci[B.off_g + f] = acc;

@@ -400,6 +400,32 @@ std::string make_source(const Engine &E, const TuneParams &tp)
     os << "    __device__ static bool radial_force(int II, int t, float r, float fc, float fcd, const float *eb, float &out)\n"
           "    {\n        switch (II * NNP_MAX_TYPES + t) {\n"
        << group_cases(ra) << "        default: return false;\n        }\n    }\n";
+    // radial sums of the symmetry-function kernel with the form fixed per case
+    {
+        bool used[16] = {};
+        for (int II = 0; II < T; ++II)
+            for (int J = 0; J < T; ++J) {
+                const DevBlockR &B = E.dpot.t[II].br[J];
+                if (B.n > 0 && B.form >= 0 && B.form < 16) used[B.form] = true;
+            }
+        os << "    template <typename Acc>\n"
+              "    __device__ static bool radial_symm(int form, const NbrView &v, const float *fcv, float rs, float eta,\n"
+              "                                       int k0, int s1, int G, Acc &acc)\n"
+              "    {\n        switch (form) {\n";
+        for (int f = 0; f < 16; ++f)
+            if (used[f])
+                os << "        case " << f << ": acc = radial_sum<" << f << ", Acc>(v, fcv, rs, eta, k0, s1, G); return true;\n";
+        os << "        default: return false;\n        }\n    }\n";
+        os << "    __device__ static bool radial_tangent(int form, const NbrView &v, const float *fcv, const float *fdv,\n"
+              "                                          const float *rr, float rs, float eta, int k0, int s1, int G,\n"
+              "                                          float &acc)\n"
+              "    {\n        switch (form) {\n";
+        for (int f = 0; f < 16; ++f)
+            if (used[f])
+                os << "        case " << f << ": acc = radial_tangent_sum<" << f
+                   << ">(v, fcv, fdv, rr, rs, eta, k0, s1, G); return true;\n";
+        os << "        default: return false;\n        }\n    }\n";
+    }
     os << "    __device__ static bool tangent(const NbrView &v, int II, int tt, const Blk &k, int cap, int lane, float *Cb)\n"
           "    {\n        switch (II * NNP_MAX_TT + tt) {\n"
        << group_cases(ta) << "        default: return false;\n        }\n    }\n};\n}  // namespace nnp\n";
