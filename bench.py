@@ -152,7 +152,7 @@ def flops_per_stage(pot, types: np.ndarray, counts: np.ndarray):
 
 # DRAM bytes per atom of one launch, from the ncu capture of the 512-structure
 # case of the batched workload (dram__bytes_read.sum + dram__bytes_write.sum / atoms)
-DRAM_BYTES_PER_ATOM = {"k_force_jit": 148.496640e6 / 134400, "k_symm_jit": 118.763776e6 / 134400}
+DRAM_BYTES_PER_ATOM = {"k_force_jit": 146.598144e6 / 134400, "k_symm_jit": 119.099648e6 / 134400}
 
 
 def traffic_bytes(kernel: str, atoms: int):
