@@ -6,7 +6,10 @@
 //   k_cell_base    exclusive scan of cells per structure
 //   k_bin          wrap atoms into their cell, count atoms per cell
 //   k_cell_start   per-structure scan of the cell counts
-//   k_fill, k_sort_cells   cell member lists, sorted by type and atom index
+//   k_fill, k_sort_cells   cell member lists, sorted by type and atom index;
+//                  the neighbour search's work items (a cell or a part of it)
+//   k_prologue_small  the steps above in one thread block, for a periodic
+//                  batch of at most 2048 atoms and 32 structures
 //   k_neigh        one block per cell or part of a cell: candidates from the
 //                  (2m+1)^3 cells gathered in shared memory, one warp per atom,
 //                  exact FP64 displacement test, neighbours grouped by type
